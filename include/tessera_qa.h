@@ -1,0 +1,161 @@
+/*
+ * tessera_qa.h -- C ABI of libtessera_qa.so, the sm_100a MPS-TEBD quantum-annealing engine.
+ *
+ * Drop-in for the reference's `tessera_qa` shared library (cuda/CMakeLists.txt:28-30),
+ * which the Rust crate links under `--features cuda` (rust/build.rs:15-19) and binds in
+ * rust/src/ffi.rs:19-35.  All pointers are caller-owned host memory, read or written only
+ * during the call; nothing is retained.  Every call is synchronous.  Calls from different
+ * host threads are safe: each thread gets its own CUDA stream and device workspace.
+ *
+ * Errors: functions returning int give 0 on success and a negative TESSERA_QA_E* code on
+ * failure; tessera_qa_anneal returns NaN.  On failure outputs are left untouched and a
+ * message is kept per thread for tessera_qa_last_error().
+ */
+#ifndef TESSERA_QA_H
+#define TESSERA_QA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define TESSERA_QA_API __attribute__((visibility("default")))
+#else
+#define TESSERA_QA_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TESSERA_QA_ABI_VERSION 1
+
+/* error codes (negative returns) */
+#define TESSERA_QA_EINVAL   (-1)  /* invalid argument: null pointer, n = 0, chi = 0, edge index out of range, NaN input */
+#define TESSERA_QA_ECUDA    (-2)  /* CUDA runtime error (no device, launch failure, out of memory) */
+#define TESSERA_QA_ESTATUS  (-3)  /* the run finished but a kernel raised a status bit (see result.status) */
+#define TESSERA_QA_ESMALL   (-4)  /* a caller buffer is too small */
+
+/* result.status bits */
+#define TESSERA_QA_ST_JACOBI_NOT_CONVERGED 1
+#define TESSERA_QA_ST_BARRIER_TIMEOUT      2
+#define TESSERA_QA_ST_BAD_DIMS             4
+#define TESSERA_QA_ST_NONFINITE            8
+
+enum tessera_qa_precision {
+    TESSERA_QA_C128 = 0, /* complex128 everywhere */
+    TESSERA_QA_C64 = 1   /* complex64 tensors and rotations; FP64 convergence test, discarded weight,
+                            entropy and energies */
+};
+
+/*
+ * Replaces the reference's only entry point, cuda/src/ffi.cpp:10-37 (bound in
+ * rust/src/ffi.rs:19-35).  Same semantics: |+>^n start, dt fixed at 0.1, one ZZ slice per
+ * step with edges in the given order, complex128, bond cap `chi`.  Writes n spins
+ * (sign of <Z_i>, ties -> +1) to out_s and, when out_entropy is not NULL, `steps` values of
+ * the qubit-0 entanglement entropy (bits).  Returns the Ising energy of the spins
+ * (E = -sum w s_i s_j - sum h s_i), or NaN on error.
+ */
+TESSERA_QA_API double tessera_qa_anneal(const double* h, size_t n, const size_t* ei, const size_t* ej, const double* ew,
+                         size_t m, const double* schedule_a, const double* schedule_b, size_t steps,
+                         size_t chi, int8_t* out_s, double* out_entropy);
+
+/* An Ising instance E(s) = -sum_e ew[e] s_ei s_ej - sum_i h_i s_i and its discretised schedule
+ * A(s_k) = schedule_a[k], B(s_k) = schedule_b[k] (rust/src/schedule.rs:8-18). */
+typedef struct tessera_qa_problem {
+    size_t n;
+    const double* h;
+    size_t m;
+    const size_t* ei;
+    const size_t* ej;
+    const double* ew;
+    size_t steps;
+    const double* schedule_a;
+    const double* schedule_b;
+} tessera_qa_problem;
+
+typedef struct tessera_qa_config {
+    double dt;              /* Trotter step; the reference's mps_anneal argument (cuda/include/mps.hpp:76-82) */
+    int zz_substeps;        /* ZZ block slices, forward/reverse alternating (cuda/src/mps.cpp:330-341) */
+    int precision;          /* enum tessera_qa_precision */
+    size_t chi;             /* bond-dimension cap */
+    double jacobi_tol;      /* rotate a column pair when |w_p^H w_q| > tol |w_p||w_q|; 0 = default */
+    int jacobi_max_sweeps;  /* 0 = default (60) */
+    int jacobi_block;       /* Jacobi column-block width (1,2,4,8,16); 0 = autotuned */
+    int device;             /* CUDA device ordinal; -1 = the calling thread's current device */
+    size_t step_begin;      /* run schedule steps [step_begin, step_end) */
+    size_t step_end;        /* 0 = problem.steps */
+    const void* initial_mps;/* NULL = |+>^n; else a checkpoint written by a previous call */
+    int skip_observables;   /* 1 = skip the final <Z>, <ZZ>, readout and prob (checkpoint runs) */
+    int reserved[7];
+} tessera_qa_config;
+
+typedef struct tessera_qa_result {
+    /* caller-provided outputs (each may be NULL) */
+    int8_t* spins;          /* n: sign(<Z_i>), ties -> +1 (cuda/src/mps.cpp:369-371) */
+    double* entropy;        /* step_end - step_begin values, qubit-0 entropy in bits */
+    void* final_mps;        /* checkpoint buffer, tessera_qa_checkpoint_bytes() bytes */
+    size_t final_mps_bytes;
+    /* filled by the call */
+    double energy;          /* Ising energy of `spins` */
+    double expected_energy; /* <psi|H_problem|psi>/<psi|psi> from the MPS */
+    double prob;            /* |<spins|psi>|^2 / <psi|psi> */
+    double max_trunc;       /* largest discarded weight ratio of any two-site update */
+    double norm2;           /* <psi|psi> */
+    long long two_site_updates;
+    int status;             /* TESSERA_QA_ST_* bits */
+    int max_sweeps;         /* most Jacobi sweeps any update used */
+    int max_bond;           /* largest bond dimension reached */
+    int reserved_i;
+    double device_ms;       /* GPU time of the Trotter steps (CUDA events) */
+    double reserved_d[4];
+} tessera_qa_result;
+
+/* Fills `cfg` with the legacy defaults: dt 0.1, zz_substeps 1, complex128, chi 32. */
+TESSERA_QA_API void tessera_qa_config_init(tessera_qa_config* cfg);
+
+/* Extended anneal: the reference's mps_anneal (cuda/src/mps.cpp:295-381) with every
+ * AnnealResult field (cuda/include/mps.hpp:37-44), a caller-chosen dt / precision, and
+ * checkpoint resume.  Returns 0 or a TESSERA_QA_E* code. */
+TESSERA_QA_API int tessera_qa_anneal_ex(const tessera_qa_problem* problem, const tessera_qa_config* config,
+                         tessera_qa_result* result);
+
+/* Bytes of a checkpoint for n sites at bond cap chi (upper bound; any dims fit). */
+TESSERA_QA_API size_t tessera_qa_checkpoint_bytes(size_t n, size_t chi);
+
+/* Thin SVD of one rows x cols complex128 matrix (row-major, interleaved re/im) through the
+ * engine's one-sided Jacobi kernel: s (min(rows,cols), descending), u (rows x k) and vh
+ * (k x cols), both row-major interleaved; u / vh may be NULL.  The counterpart of the
+ * reference's tessera::svd (cuda/src/linalg.cpp:107-172). */
+TESSERA_QA_API int tessera_qa_svd(const double* a, size_t rows, size_t cols, double* s, double* u, double* vh);
+
+/* Copies the calling thread's last error message into buf; returns its full length. */
+TESSERA_QA_API int tessera_qa_last_error(char* buf, size_t len);
+
+/* ---- sessions: device-resident anneal state (no host copies between calls) ---- */
+typedef struct tessera_qa_session tessera_qa_session;
+
+/* Uploads the problem and allocates the MPS at bond cap config->chi; state |+>^n. */
+TESSERA_QA_API tessera_qa_session* tessera_qa_session_create(const tessera_qa_problem* problem,
+                                              const tessera_qa_config* config);
+/* Replaces the state by a seeded random MPS with every bond at its cap (min(chi, 2^i,
+ * 2^(n-i))), sites scaled so theta stays O(1). */
+TESSERA_QA_API int tessera_qa_session_randomize(tessera_qa_session* s, uint64_t seed);
+/* Enqueues Trotter steps [step_begin, step_begin + nsteps) on the session's stream; returns
+ * without waiting. */
+TESSERA_QA_API int tessera_qa_session_run(tessera_qa_session* s, size_t step_begin, size_t nsteps);
+/* The session's cudaStream_t. */
+TESSERA_QA_API void* tessera_qa_session_stream(tessera_qa_session* s);
+/* Waits for the stream and fills counters (updates, max_trunc, status, sweeps, bonds). */
+TESSERA_QA_API int tessera_qa_session_sync(tessera_qa_session* s, tessera_qa_result* result);
+/* Final observables of the current state into result (like tessera_qa_anneal_ex). */
+TESSERA_QA_API int tessera_qa_session_observe(tessera_qa_session* s, tessera_qa_result* result);
+/* Writes / reads a checkpoint of the current state. */
+TESSERA_QA_API int tessera_qa_session_save(tessera_qa_session* s, void* buf, size_t bytes);
+TESSERA_QA_API int tessera_qa_session_load(tessera_qa_session* s, const void* buf, size_t bytes);
+TESSERA_QA_API void tessera_qa_session_destroy(tessera_qa_session* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TESSERA_QA_H */

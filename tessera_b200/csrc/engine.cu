@@ -1,0 +1,843 @@
+// engine.cu -- host orchestration of the anneal and the C ABI of libtessera_qa.so.
+//
+// One Engine<T> owns one instance's device state (a single cudaMalloc arena) and a CUDA
+// stream.  A Trotter step (cuda/src/mps.cpp:309-356) is enqueued without any host wait:
+//   K5 single-site half step (all sites, one launch)
+//   for every ZZ gate of the step, in the reference's order, expanded through the swap
+//   network (cuda/src/mps.cpp:126-145, 330-341): K1 theta -> K2/K3 Jacobi SVD + keep rule
+//   -> K4 absorb
+//   K5 single-site half step
+//   K6 right-environment chain to bond 1 + qubit-0 entropy
+// Bond dimensions live on the device; the host only tracks upper bounds
+// (dim_{i+1} <= min(chi, 2 dim_i, 2 dim_{i+2})) to size the grids.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/tessera_qa.h"
+#include "engine.cuh"
+
+namespace tq {
+
+#define TQ_CK(x)                                                                               \
+    do {                                                                                       \
+        cudaError_t e_ = (x);                                                                  \
+        if (e_ != cudaSuccess)                                                                 \
+            throw CudaError(std::string("CUDA: ") + cudaGetErrorString(e_) + " (" #x ")");      \
+    } while (0)
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct ArgError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+static thread_local std::string t_err;
+
+static void set_err(const std::string& s) { t_err = s; }
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// ---------------------------------------------------------------------------------
+// small kernels local to the orchestrator
+// ---------------------------------------------------------------------------------
+__global__ void k_set_int(int* p, int v) { *p = v; }
+
+template <typename T>
+__global__ void k_random_sites(MpsView<T> mps, unsigned long long seed) {
+    using V = cplx_t<T>;
+    const int i = blockIdx.y;
+    const int dl = mps.dims[i], dr = mps.dims[i + 1];
+    const long long tot = (long long)dl * 2 * dr;
+    const double scale = 1.0 / sqrt(2.0 * dl);
+    V* S = mps.site(i);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+        const long long row = t / dr, b = t - row * dr;
+        unsigned long long z = seed ^ ((unsigned long long)i << 40) ^ (unsigned long long)t * 0x9E3779B97F4A7C15ull;
+        // splitmix64, twice
+        unsigned long long u[2];
+        for (int q = 0; q < 2; ++q) {
+            z += 0x9E3779B97F4A7C15ull;
+            unsigned long long x = z;
+            x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+            x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+            u[q] = x ^ (x >> 31);
+        }
+        const double u1 = ((u[0] >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+        const double u2 = (u[1] >> 11) * (1.0 / 9007199254740992.0);
+        const double r = sqrt(-2.0 * log(u1)) * scale;
+        S[row * mps.cap + b] = mk<V>((T)(r * cos(6.283185307179586 * u2)), (T)(r * sin(6.283185307179586 * u2)));
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Engine
+// ---------------------------------------------------------------------------------
+struct ProblemHost {
+    int n = 0, m = 0, steps = 0;
+    std::vector<double> h, w, sa, sb;
+    std::vector<int> ei, ej;
+};
+
+static ProblemHost validate_problem(const tessera_qa_problem* p) {
+    if (!p) throw ArgError("problem is NULL");
+    if (p->n == 0) throw ArgError("n must be >= 1");
+    if (p->n > 4096) throw ArgError("n > 4096 is not supported");
+    if (!p->h) throw ArgError("h is NULL");
+    if (p->m && (!p->ei || !p->ej || !p->ew)) throw ArgError("edge arrays are NULL");
+    if (p->steps && (!p->schedule_a || !p->schedule_b)) throw ArgError("schedule arrays are NULL");
+    ProblemHost P;
+    P.n = (int)p->n;
+    P.m = (int)p->m;
+    P.steps = (int)p->steps;
+    P.h.assign(p->h, p->h + p->n);
+    for (double x : P.h)
+        if (!std::isfinite(x)) throw ArgError("h contains NaN/Inf");
+    for (size_t e = 0; e < p->m; ++e) {
+        if (p->ei[e] >= p->n || p->ej[e] >= p->n) throw ArgError("edge index out of range");
+        if (!std::isfinite(p->ew[e])) throw ArgError("ew contains NaN/Inf");
+        P.ei.push_back((int)p->ei[e]);
+        P.ej.push_back((int)p->ej[e]);
+        P.w.push_back(p->ew[e]);
+    }
+    P.sa.assign(p->schedule_a, p->schedule_a + p->steps);
+    P.sb.assign(p->schedule_b, p->schedule_b + p->steps);
+    for (size_t k = 0; k < p->steps; ++k)
+        if (!std::isfinite(P.sa[k]) || !std::isfinite(P.sb[k])) throw ArgError("schedule contains NaN/Inf");
+    return P;
+}
+
+struct Config {
+    double dt = 0.1;
+    int ns = 1;
+    int precision = TESSERA_QA_C128;
+    int chi = 32;
+    double tol = 0.0;
+    int max_sweeps = 60;
+    int block = 0;
+    int device = -1;
+    int min_ld = 0;  // workspace rows/cols at least this (standalone SVD)
+};
+
+static Config validate_config(const tessera_qa_config* c) {
+    Config C;
+    if (!c) return C;
+    if (!(c->dt > 0) || !std::isfinite(c->dt)) throw ArgError("dt must be a finite positive number");
+    if (c->chi == 0) throw ArgError("chi must be >= 1");
+    if (c->chi > 1024) throw ArgError("chi > 1024 is not supported");
+    if (c->precision != TESSERA_QA_C128 && c->precision != TESSERA_QA_C64) throw ArgError("unknown precision");
+    if (c->jacobi_block && !(c->jacobi_block == 1 || c->jacobi_block == 2 || c->jacobi_block == 4 ||
+                             c->jacobi_block == 8 || c->jacobi_block == 16))
+        throw ArgError("jacobi_block must be 0, 1, 2, 4, 8 or 16");
+    if (c->jacobi_max_sweeps < 0 || c->jacobi_max_sweeps > 1000) throw ArgError("jacobi_max_sweeps out of range");
+    C.dt = c->dt;
+    C.ns = c->zz_substeps < 1 ? 1 : c->zz_substeps;
+    C.precision = c->precision;
+    C.chi = (int)c->chi;
+    C.tol = c->jacobi_tol;
+    C.max_sweeps = c->jacobi_max_sweeps ? c->jacobi_max_sweeps : 60;
+    C.block = c->jacobi_block;
+    C.device = c->device;
+    return C;
+}
+
+class EngineBase {
+public:
+    virtual ~EngineBase() = default;
+    virtual void init_plus() = 0;
+    virtual void randomize(unsigned long long seed) = 0;
+    virtual void run(int k0, int k1) = 0;
+    virtual void sync_stats(tessera_qa_result* r) = 0;
+    virtual void observe(tessera_qa_result* r) = 0;
+    virtual size_t save(void* buf, size_t bytes, unsigned long long step_next) = 0;
+    virtual void load(const void* buf, size_t bytes) = 0;
+    virtual void copy_entropy(double* out, int k0, int k1) = 0;
+    virtual cudaStream_t stream() const = 0;
+    virtual double last_ms() const = 0;
+};
+
+// checkpoint layout: "TQMPSv1\0", u32 n, u32 0, u64 step_next, u64 0, i32 dims[n+1] (8-byte padded),
+// then site tensors (Dl, 2, Dr) as complex128, (a, s, b) row-major.
+static const char kMagic[8] = {'T', 'Q', 'M', 'P', 'S', 'v', '1', 0};
+static size_t ckpt_header_bytes(int n) { return 32 + ((size_t)4 * (n + 1) + 7) / 8 * 8; }
+
+template <typename T>
+class Engine final : public EngineBase {
+    using V = cplx_t<T>;
+
+public:
+    Engine(const ProblemHost& P, const Config& C) : P_(P), C_(C) {
+        n_ = P.n;
+        m_ = P.m;
+        // bond cap: min(chi, 2^floor(n/2)), the largest bond any n-site chain can need
+        long long full = 1;
+        for (int q = 0; q < n_ / 2 && full < C.chi; ++q) full <<= 1;
+        cap_ = (int)std::min<long long>(C.chi, full);
+        if (cap_ < 1) cap_ = 1;
+        ld_ = std::max(2 * cap_, (C.min_ld + 7) & ~7);
+        build_ops();
+        allocate();
+        TQ_CK(cudaEventCreate(&ev0_));
+        TQ_CK(cudaEventCreate(&ev1_));
+        upload_problem();
+        init_plus();
+    }
+    ~Engine() override {
+        if (stream_) cudaStreamSynchronize(stream_);
+        if (ev0_) cudaEventDestroy(ev0_);
+        if (ev1_) cudaEventDestroy(ev1_);
+        if (base_) cudaFree(base_);
+        if (stream_) cudaStreamDestroy(stream_);
+    }
+
+    cudaStream_t stream() const override { return stream_; }
+    double last_ms() const override { return last_ms_; }
+
+    void init_plus() override {
+        launch_init_plus<T>(mps(), stream_);
+        TQ_CK(cudaMemsetAsync(stats_, 0, sizeof(RunStats), stream_));
+        std::fill(ub_.begin(), ub_.end(), 1);
+    }
+
+    void randomize(unsigned long long seed) override {
+        std::vector<int> d(n_ + 1, 1);
+        for (int i = 1; i < n_; ++i) {
+            long long a = 1, b = 1;
+            for (int q = 0; q < i && a < cap_; ++q) a <<= 1;
+            for (int q = 0; q < n_ - i && b < cap_; ++q) b <<= 1;
+            d[i] = (int)std::min<long long>(cap_, std::min(a, b));
+        }
+        TQ_CK(cudaMemcpyAsync(dims_, d.data(), sizeof(int) * (n_ + 1), cudaMemcpyHostToDevice, stream_));
+        TQ_CK(cudaStreamSynchronize(stream_));
+        k_random_sites<T><<<dim3(64, n_), 256, 0, stream_>>>(mps(), seed);
+        TQ_CK(cudaGetLastError());
+        TQ_CK(cudaMemsetAsync(stats_, 0, sizeof(RunStats), stream_));
+        ub_ = d;
+    }
+
+    void run(int k0, int k1) override {
+        if (k0 < 0 || k1 > P_.steps || k0 > k1) throw ArgError("step range outside the schedule");
+        k_set_int<<<1, 1, 0, stream_>>>(step_, k0);
+        TQ_CK(cudaGetLastError());
+        TQ_CK(cudaEventRecord(ev0_, stream_));
+        const ScheduleView sch = schedule();
+        const MpsView<T> M = mps();
+        for (int k = k0; k < k1; ++k) {
+            single_site(sch);
+            for (const GateOp& op : ops_) two_site(M, sch, op);
+            single_site(sch);
+            entropy_step(M);
+            launch_step_inc(step_, stream_);
+        }
+        TQ_CK(cudaEventRecord(ev1_, stream_));
+        ran_ = true;
+    }
+
+    void sync_stats(tessera_qa_result* r) override {
+        TQ_CK(cudaStreamSynchronize(stream_));
+        TQ_CK(cudaGetLastError());
+        RunStats st;
+        TQ_CK(cudaMemcpy(&st, stats_, sizeof(st), cudaMemcpyDeviceToHost));
+        if (ran_) {
+            float ms = 0;
+            TQ_CK(cudaEventElapsedTime(&ms, ev0_, ev1_));
+            last_ms_ = ms;
+        }
+        if (r) {
+            r->max_trunc = st.max_trunc;
+            r->two_site_updates = st.updates;
+            r->status = st.status;
+            r->max_sweeps = st.max_sweeps;
+            r->max_bond = std::max(st.max_bond, 1);
+            r->device_ms = last_ms_;
+        }
+    }
+
+    void copy_entropy(double* out, int k0, int k1) override {
+        if (!out || k1 <= k0) return;
+        TQ_CK(cudaMemcpyAsync(out, entropy_ + k0, sizeof(double) * (k1 - k0), cudaMemcpyDeviceToHost, stream_));
+        TQ_CK(cudaStreamSynchronize(stream_));
+    }
+
+    // <Z_i>, <Z_i Z_j>, <psi|psi>, readout, prob (cuda/src/mps.cpp:358-380).
+    void observe(tessera_qa_result* r) override {
+        const MpsView<T> M = mps();
+        launch_chain<T>(M, 1, obsR_, n_, envs_, xs_, bar_, stats_, cap_, stream_);
+        launch_chain<T>(M, 0, obsL_, n_obsL_, envs_, xs_, bar_, stats_, cap_, stream_);
+        launch_pair_dots<T>(M, envs_, dots_, 1 + n_ + m_, dotout_, stream_);
+        std::vector<double> v(1 + n_ + m_);
+        TQ_CK(cudaMemcpyAsync(v.data(), dotout_, sizeof(double) * v.size(), cudaMemcpyDeviceToHost, stream_));
+        TQ_CK(cudaStreamSynchronize(stream_));
+        const double nrm = v[0];
+        std::vector<double> ez(n_), ezz(m_);
+        for (int i = 0; i < n_; ++i) ez[i] = nrm > 0 ? v[1 + i] / nrm : 0.0;
+        for (int e = 0; e < m_; ++e) ezz[e] = nrm > 0 ? v[1 + n_ + e] / nrm : 0.0;
+        double eexp = 0.0;
+        for (int e = 0; e < m_; ++e) eexp -= P_.w[e] * ezz[e];
+        for (int i = 0; i < n_; ++i) eexp -= P_.h[i] * ez[i];
+        std::vector<int8_t> spins(n_);
+        for (int i = 0; i < n_; ++i) spins[i] = ez[i] >= 0.0 ? 1 : -1;
+        double E = 0.0;
+        for (int e = 0; e < m_; ++e) E -= P_.w[e] * spins[P_.ei[e]] * spins[P_.ej[e]];
+        for (int i = 0; i < n_; ++i) E -= P_.h[i] * spins[i];
+        TQ_CK(cudaMemcpyAsync(spins_d_, spins.data(), n_, cudaMemcpyHostToDevice, stream_));
+        launch_amplitude<T>(M, spins_d_, vbuf_, amp2_, stream_);
+        double a2 = 0;
+        TQ_CK(cudaMemcpyAsync(&a2, amp2_, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        TQ_CK(cudaStreamSynchronize(stream_));
+        if (r) {
+            r->energy = E;
+            r->expected_energy = eexp;
+            r->prob = nrm > 0 ? a2 / nrm : 0.0;
+            r->norm2 = nrm;
+            if (r->spins) std::memcpy(r->spins, spins.data(), n_);
+        }
+    }
+
+    size_t save(void* buf, size_t bytes, unsigned long long step_next) override {
+        TQ_CK(cudaStreamSynchronize(stream_));
+        std::vector<int> d(n_ + 1);
+        TQ_CK(cudaMemcpy(d.data(), dims_, sizeof(int) * (n_ + 1), cudaMemcpyDeviceToHost));
+        size_t need = ckpt_header_bytes(n_);
+        for (int i = 0; i < n_; ++i) need += (size_t)d[i] * 2 * d[i + 1] * 16;
+        if (!buf || bytes < need) throw ArgError("checkpoint buffer too small");
+        char* p = static_cast<char*>(buf);
+        std::memset(p, 0, ckpt_header_bytes(n_));
+        std::memcpy(p, kMagic, 8);
+        const uint32_t nn = (uint32_t)n_;
+        std::memcpy(p + 8, &nn, 4);
+        std::memcpy(p + 16, &step_next, 8);
+        std::memcpy(p + 32, d.data(), sizeof(int) * (n_ + 1));
+        char* q = p + ckpt_header_bytes(n_);
+        std::vector<V> tmp;
+        for (int i = 0; i < n_; ++i) {
+            const size_t rows = (size_t)2 * d[i], cols = d[i + 1];
+            tmp.resize(rows * cols);
+            TQ_CK(cudaMemcpy2D(tmp.data(), cols * sizeof(V), sites_ + (size_t)i * site_stride(), cap_ * sizeof(V),
+                               cols * sizeof(V), rows, cudaMemcpyDeviceToHost));
+            double* o = reinterpret_cast<double*>(q);
+            for (size_t e = 0; e < rows * cols; ++e) {
+                const double re = (double)tmp[e].x, im = (double)tmp[e].y;
+                std::memcpy(o + 2 * e, &re, 8);
+                std::memcpy(o + 2 * e + 1, &im, 8);
+            }
+            q += rows * cols * 16;
+        }
+        return need;
+    }
+
+    void load(const void* buf, size_t bytes) override {
+        const char* p = static_cast<const char*>(buf);
+        if (!p || bytes < 32 || std::memcmp(p, kMagic, 8) != 0) throw ArgError("not a tessera_qa checkpoint");
+        uint32_t nn;
+        std::memcpy(&nn, p + 8, 4);
+        if ((int)nn != n_) throw ArgError("checkpoint has a different number of sites");
+        if (bytes < ckpt_header_bytes(n_)) throw ArgError("checkpoint truncated");
+        std::vector<int> d(n_ + 1);
+        std::memcpy(d.data(), p + 32, sizeof(int) * (n_ + 1));
+        if (d[0] != 1 || d[n_] != 1) throw ArgError("checkpoint end bonds must be 1");
+        size_t need = ckpt_header_bytes(n_);
+        for (int i = 0; i <= n_; ++i)
+            if (d[i] < 1 || d[i] > cap_) throw ArgError("checkpoint bond dimension exceeds this run's cap");
+        for (int i = 0; i < n_; ++i) need += (size_t)d[i] * 2 * d[i + 1] * 16;
+        if (bytes < need) throw ArgError("checkpoint truncated");
+        TQ_CK(cudaStreamSynchronize(stream_));
+        TQ_CK(cudaMemcpy(dims_, d.data(), sizeof(int) * (n_ + 1), cudaMemcpyHostToDevice));
+        const char* q = p + ckpt_header_bytes(n_);
+        std::vector<V> tmp;
+        for (int i = 0; i < n_; ++i) {
+            const size_t rows = (size_t)2 * d[i], cols = d[i + 1];
+            tmp.resize(rows * cols);
+            const double* src = reinterpret_cast<const double*>(q);
+            for (size_t e = 0; e < rows * cols; ++e) {
+                double re, im;
+                std::memcpy(&re, src + 2 * e, 8);
+                std::memcpy(&im, src + 2 * e + 1, 8);
+                tmp[e] = mk<V>((T)re, (T)im);
+            }
+            TQ_CK(cudaMemcpy2D(sites_ + (size_t)i * site_stride(), cap_ * sizeof(V), tmp.data(), cols * sizeof(V),
+                               cols * sizeof(V), rows, cudaMemcpyHostToDevice));
+            q += rows * cols * 16;
+        }
+        TQ_CK(cudaMemset(stats_, 0, sizeof(RunStats)));
+        ub_ = d;
+    }
+
+    // standalone SVD of an R x N matrix (column-major in W) -> perm, sig
+    void svd_only(const std::vector<V>& colmajor, int R, int N, std::vector<int>& perm, std::vector<double>& sig,
+                  std::vector<V>& Wout) {
+        TQ_CK(cudaMemcpy2DAsync(W_, ld_ * sizeof(V), colmajor.data(), R * sizeof(V), R * sizeof(V), N,
+                                cudaMemcpyHostToDevice, stream_));
+        const int bw = pick_block(R, N);
+        launch_svd<T>(mps(), 0, std::min(R, N), tol_for(R), C_.max_sweeps, work(), R, N, bw, stream_, R, N);
+        const int k = std::min(R, N);
+        perm.resize(k);
+        sig.resize(k);
+        Wout.resize((size_t)R * N);
+        TQ_CK(cudaMemcpyAsync(perm.data(), perm_, sizeof(int) * k, cudaMemcpyDeviceToHost, stream_));
+        TQ_CK(cudaMemcpyAsync(sig.data(), sig_, sizeof(double) * k, cudaMemcpyDeviceToHost, stream_));
+        TQ_CK(cudaMemcpy2DAsync(Wout.data(), R * sizeof(V), W_, ld_ * sizeof(V), R * sizeof(V), N,
+                                cudaMemcpyDeviceToHost, stream_));
+        TQ_CK(cudaStreamSynchronize(stream_));
+        RunStats st;
+        TQ_CK(cudaMemcpy(&st, stats_, sizeof(st), cudaMemcpyDeviceToHost));
+        status_ = st.status;
+    }
+    int status_ = 0;
+    int cap() const { return cap_; }
+
+private:
+    ProblemHost P_;
+    Config C_;
+    int n_ = 0, m_ = 0, cap_ = 1, ld_ = 2;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    char* base_ = nullptr;
+    V *sites_ = nullptr, *theta_ = nullptr, *W_ = nullptr, *envs_ = nullptr, *xs_ = nullptr, *vbuf_ = nullptr;
+    int *dims_ = nullptr, *perm_ = nullptr, *counters_ = nullptr, *step_ = nullptr;
+    double *sig2_ = nullptr, *sig_ = nullptr, *h_ = nullptr, *w_ = nullptr, *sa_ = nullptr, *sb_ = nullptr;
+    double *entropy_ = nullptr, *dotout_ = nullptr, *amp2_ = nullptr;
+    int8_t* spins_d_ = nullptr;
+    GridBar* bar_ = nullptr;
+    RunStats* stats_ = nullptr;
+    ChainStep *entc_ = nullptr, *obsR_ = nullptr, *obsL_ = nullptr;
+    PairDot* dots_ = nullptr;
+    int n_ent_ = 0, n_obsL_ = 0;
+    long long r1_off_ = 0;
+    std::vector<GateOp> ops_;
+    std::vector<int> ub_;
+    bool ran_ = false;
+    double last_ms_ = 0.0;
+
+    size_t site_stride() const { return (size_t)2 * cap_ * cap_; }
+    MpsView<T> mps() const { return MpsView<T>{sites_, dims_, n_, cap_, (long long)site_stride()}; }
+    ScheduleView schedule() const { return ScheduleView{h_, w_, sa_, sb_, step_, C_.dt, C_.dt / C_.ns}; }
+    SvdWork<T> work() const { return SvdWork<T>{theta_, W_, ld_, sig2_, sig_, perm_, counters_, bar_, stats_}; }
+
+    double tol_for(int R) const {
+        if (C_.tol > 0) return C_.tol;
+        const double eps = sizeof(T) == 8 ? 2.220446049250313e-16 : 1.1920928955078125e-07;
+        return sizeof(T) == 8 ? std::max(R, 16) * eps : 8.0 * std::sqrt((double)std::max(R, 16)) * eps;
+    }
+
+    int pick_block(int R, int N) const {
+        int b = C_.block;
+        if (!b) {
+            // default schedule: wide blocks for small matrices (few grid barriers), narrower
+            // ones for large matrices (enough block pairs to fill the SMs)
+            if (N <= 32) b = 16;
+            else if (N <= 128) b = 8;
+            else if (N <= 512) b = 4;
+            else b = 4;
+        }
+        const int rows_cap = (R + 7) & ~7;
+        while (b > 1 && (size_t)2 * b * rows_cap * sizeof(V) > 200 * 1024) b >>= 1;
+        return b;
+    }
+
+    void build_ops() {
+        // ZZ block of one step (cuda/src/mps.cpp:330-341) expanded through the swap network
+        // (cuda/src/mps.cpp:126-145).
+        ops_.clear();
+        for (int s = 0; s < C_.ns; ++s) {
+            for (int q = 0; q < m_; ++q) {
+                const int e = (s % 2 == 0) ? q : m_ - 1 - q;
+                int i = P_.ei[e], j = P_.ej[e];
+                if (i > j) std::swap(i, j);
+                if (i == j) continue;
+                for (int k = j; k > i + 1; --k) ops_.push_back(GateOp{k - 1, GATE_SWAP, e, 0});
+                ops_.push_back(GateOp{i, GATE_ZZ, e, 0});
+                for (int k = i + 1; k < j; ++k) ops_.push_back(GateOp{k, GATE_SWAP, e, 0});
+            }
+        }
+        ub_.assign(n_ + 1, 1);
+    }
+
+    void allocate() {
+        const size_t es = sizeof(V);
+        const size_t unit = (size_t)cap_ * cap_;
+        const long long NE = 3 + 3LL * n_ + m_;
+        // observable chain: L (n) + Z (n) + ZZ chains
+        n_obsL_ = 2 * n_;
+        for (int e = 0; e < m_; ++e) {
+            const int i = std::min(P_.ei[e], P_.ej[e]), j = std::max(P_.ei[e], P_.ej[e]);
+            if (i != j) n_obsL_ += j - i + 1;
+        }
+        n_ent_ = std::max(0, n_ - 1);
+        struct Item { void** p; size_t bytes; };
+        size_t off = 0;
+        std::vector<std::pair<size_t, void**>> plan;
+        auto add = [&](void** p, size_t bytes) { plan.push_back({off, p}); off += align256(std::max<size_t>(bytes, 8)); };
+        add((void**)&sites_, es * site_stride() * n_);
+        add((void**)&dims_, sizeof(int) * (n_ + 1));
+        add((void**)&theta_, es * (size_t)ld_ * ld_);
+        add((void**)&W_, es * (size_t)ld_ * ld_);
+        add((void**)&sig2_, sizeof(double) * ld_);
+        add((void**)&sig_, sizeof(double) * ld_);
+        add((void**)&perm_, sizeof(int) * ld_);
+        add((void**)&counters_, sizeof(int) * C_.max_sweeps);
+        add((void**)&bar_, sizeof(GridBar));
+        add((void**)&stats_, sizeof(RunStats));
+        add((void**)&h_, sizeof(double) * n_);
+        add((void**)&w_, sizeof(double) * std::max(m_, 1));
+        add((void**)&sa_, sizeof(double) * std::max(P_.steps, 1));
+        add((void**)&sb_, sizeof(double) * std::max(P_.steps, 1));
+        add((void**)&step_, sizeof(int));
+        add((void**)&entropy_, sizeof(double) * std::max(P_.steps, 1));
+        add((void**)&envs_, es * unit * NE);
+        add((void**)&xs_, es * unit * 4);  // chain phase-1 product, up to (2 cap) x (2 cap)
+        add((void**)&vbuf_, es * (size_t)2 * cap_);
+        add((void**)&entc_, sizeof(ChainStep) * std::max(n_ent_, 1));
+        add((void**)&obsR_, sizeof(ChainStep) * n_);
+        add((void**)&obsL_, sizeof(ChainStep) * n_obsL_);
+        add((void**)&dots_, sizeof(PairDot) * (1 + n_ + m_));
+        add((void**)&dotout_, sizeof(double) * (1 + n_ + m_));
+        add((void**)&amp2_, sizeof(double));
+        add((void**)&spins_d_, n_);
+        TQ_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        TQ_CK(cudaMalloc(&base_, off));
+        for (auto& it : plan) *it.second = base_ + it.first;
+        TQ_CK(cudaMemsetAsync(bar_, 0, sizeof(GridBar), stream_));
+        TQ_CK(cudaMemsetAsync(stats_, 0, sizeof(RunStats), stream_));
+        TQ_CK(cudaMemsetAsync(entropy_, 0, sizeof(double) * std::max(P_.steps, 1), stream_));
+        TQ_CK(cudaMemsetAsync(envs_, 0, es * unit, stream_));  // the ONE env
+        V one = mk<V>(1, 0);
+        TQ_CK(cudaMemcpyAsync(envs_, &one, sizeof(V), cudaMemcpyHostToDevice, stream_));
+        // chain step lists
+        const long long U = (long long)unit;
+        auto Loff = [&](int i) { return i == 0 ? 0LL : (1LL + i) * U; };
+        auto Roff = [&](int i) { return i == n_ ? 0LL : (1LL + n_ + i) * U; };
+        auto Zoff = [&](int i) { return (1LL + 2LL * n_ + i) * U; };
+        auto ZZoff = [&](int e) { return (1LL + 3LL * n_ + e) * U; };
+        const long long T0 = (1LL + 3LL * n_ + m_) * U, T1 = T0 + U;
+        std::vector<ChainStep> ent;
+        for (int q = 0; q < n_ent_; ++q) {
+            const int site = n_ - 1 - q;
+            ent.push_back(ChainStep{site, 0, q == 0 ? 0LL : ((q - 1) & 1 ? T1 : T0), (q & 1) ? T1 : T0});
+        }
+        r1_off_ = n_ent_ ? (((n_ent_ - 1) & 1) ? T1 : T0) : 0;
+        std::vector<ChainStep> R, L;
+        for (int q = 0; q < n_; ++q) {
+            const int site = n_ - 1 - q;
+            R.push_back(ChainStep{site, 0, Roff(site + 1), Roff(site)});
+        }
+        for (int i = 0; i < n_; ++i) L.push_back(ChainStep{i, 0, Loff(i), Loff(i + 1)});
+        for (int i = 0; i < n_; ++i) L.push_back(ChainStep{i, 1, Loff(i), Zoff(i)});
+        std::vector<PairDot> D;
+        D.push_back(PairDot{Loff(n_), 0, n_, 0});
+        for (int i = 0; i < n_; ++i) D.push_back(PairDot{Zoff(i), Roff(i + 1), i + 1, 0});
+        for (int e = 0; e < m_; ++e) {
+            const int i = std::min(P_.ei[e], P_.ej[e]), j = std::max(P_.ei[e], P_.ej[e]);
+            if (i == j) {
+                // the reference's expect_zz(i, i) inserts Z once (cuda/src/mps.cpp:156,188-194)
+                D.push_back(PairDot{Zoff(i), Roff(i + 1), i + 1, 0});
+                continue;
+            }
+            long long cur = Loff(i);
+            int flip = 0;
+            for (int s = i; s <= j; ++s) {
+                const bool last = (s == j);
+                const long long out = last ? ZZoff(e) : (flip ? T1 : T0);
+                L.push_back(ChainStep{s, (s == i || s == j) ? 1 : 0, cur, out});
+                cur = out;
+                flip ^= 1;
+            }
+            D.push_back(PairDot{ZZoff(e), Roff(j + 1), j + 1, 0});
+        }
+        if (!ent.empty())
+            TQ_CK(cudaMemcpyAsync(entc_, ent.data(), sizeof(ChainStep) * ent.size(), cudaMemcpyHostToDevice, stream_));
+        TQ_CK(cudaMemcpyAsync(obsR_, R.data(), sizeof(ChainStep) * R.size(), cudaMemcpyHostToDevice, stream_));
+        TQ_CK(cudaMemcpyAsync(obsL_, L.data(), sizeof(ChainStep) * L.size(), cudaMemcpyHostToDevice, stream_));
+        TQ_CK(cudaMemcpyAsync(dots_, D.data(), sizeof(PairDot) * D.size(), cudaMemcpyHostToDevice, stream_));
+        TQ_CK(cudaStreamSynchronize(stream_));
+    }
+
+    void upload_problem() {
+        TQ_CK(cudaMemcpyAsync(h_, P_.h.data(), sizeof(double) * n_, cudaMemcpyHostToDevice, stream_));
+        if (m_) TQ_CK(cudaMemcpyAsync(w_, P_.w.data(), sizeof(double) * m_, cudaMemcpyHostToDevice, stream_));
+        if (P_.steps) {
+            TQ_CK(cudaMemcpyAsync(sa_, P_.sa.data(), sizeof(double) * P_.steps, cudaMemcpyHostToDevice, stream_));
+            TQ_CK(cudaMemcpyAsync(sb_, P_.sb.data(), sizeof(double) * P_.steps, cudaMemcpyHostToDevice, stream_));
+        }
+        TQ_CK(cudaStreamSynchronize(stream_));
+    }
+
+    void single_site(const ScheduleView& sch) {
+        int mx = 1;
+        for (int i = 0; i < n_; ++i) mx = std::max(mx, ub_[i] * ub_[i + 1]);
+        launch_single_site<T>(mps(), sch, mx, stream_);
+    }
+
+    void two_site(const MpsView<T>& M, const ScheduleView& sch, const GateOp& op) {
+        const int i = op.bond;
+        const int dl = ub_[i], dr = ub_[i + 2];
+        const int keep_ub = std::min(C_.chi, std::min(2 * dl, 2 * dr));
+        launch_theta<T>(M, sch, op, nullptr, work(), dl, dr, stream_);
+        launch_svd<T>(M, i, C_.chi, tol_for(2 * dl), C_.max_sweeps, work(), 2 * dl, 2 * dr, pick_block(2 * dl, 2 * dr),
+                      stream_);
+        launch_absorb<T>(M, i, work(), 2 * dl, 2 * dr, keep_ub, stream_);
+        ub_[i + 1] = keep_ub;
+    }
+
+    void entropy_step(const MpsView<T>& M) {
+        if (n_ >= 2) {
+            launch_chain<T>(M, 1, entc_, n_ent_, envs_, xs_, bar_, stats_, cap_, stream_);
+            launch_entropy<T>(M, envs_ + r1_off_, entropy_, step_, stream_);
+        } else {
+            launch_entropy<T>(M, nullptr, entropy_, step_, stream_);
+        }
+    }
+};
+
+static std::unique_ptr<EngineBase> make_engine(const ProblemHost& P, const Config& C) {
+    if (C.device >= 0) TQ_CK(cudaSetDevice(C.device));
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw CudaError("no CUDA device available");
+    if (C.precision == TESSERA_QA_C64) return std::unique_ptr<EngineBase>(new Engine<float>(P, C));
+    return std::unique_ptr<EngineBase>(new Engine<double>(P, C));
+}
+
+}  // namespace tq
+
+using namespace tq;
+
+struct tessera_qa_session {
+    std::unique_ptr<EngineBase> eng;
+    ProblemHost P;
+    Config C;
+};
+
+template <typename F>
+static int guarded(F&& f) {
+    try {
+        return f();
+    } catch (const ArgError& e) {
+        set_err(e.what());
+        return TESSERA_QA_EINVAL;
+    } catch (const CudaError& e) {
+        set_err(e.what());
+        return TESSERA_QA_ECUDA;
+    } catch (const std::exception& e) {
+        set_err(std::string("CUDA: ") + e.what());
+        return TESSERA_QA_ECUDA;
+    }
+}
+
+extern "C" {
+
+void tessera_qa_config_init(tessera_qa_config* cfg) {
+    if (!cfg) return;
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->dt = 0.1;
+    cfg->zz_substeps = 1;
+    cfg->precision = TESSERA_QA_C128;
+    cfg->chi = 32;
+    cfg->device = -1;
+}
+
+size_t tessera_qa_checkpoint_bytes(size_t n, size_t chi) {
+    return ckpt_header_bytes((int)n) + n * 2 * chi * chi * 16;
+}
+
+int tessera_qa_last_error(char* buf, size_t len) {
+    if (buf && len) {
+        const size_t k = std::min(len - 1, t_err.size());
+        std::memcpy(buf, t_err.data(), k);
+        buf[k] = 0;
+    }
+    return (int)t_err.size();
+}
+
+int tessera_qa_anneal_ex(const tessera_qa_problem* problem, const tessera_qa_config* config,
+                         tessera_qa_result* result) {
+    return guarded([&]() -> int {
+        if (!result) throw ArgError("result is NULL");
+        ProblemHost P = validate_problem(problem);
+        Config C = validate_config(config);
+        const int k0 = config ? (int)config->step_begin : 0;
+        const int k1 = (config && config->step_end) ? (int)config->step_end : P.steps;
+        if (k0 > k1 || k1 > P.steps) throw ArgError("step range outside the schedule");
+        auto eng = make_engine(P, C);
+        if (config && config->initial_mps)
+            eng->load(config->initial_mps, (size_t)-1 / 2);
+        eng->run(k0, k1);
+        tessera_qa_result r = *result;
+        eng->sync_stats(&r);
+        if (!(config && config->skip_observables)) eng->observe(&r);
+        if (r.entropy) eng->copy_entropy(r.entropy, k0, k1);
+        if (r.final_mps) eng->save(r.final_mps, r.final_mps_bytes, (unsigned long long)k1);
+        *result = r;
+        if (r.status) {
+            set_err("kernel status bits set: " + std::to_string(r.status));
+            return TESSERA_QA_ESTATUS;
+        }
+        return 0;
+    });
+}
+
+double tessera_qa_anneal(const double* h, size_t n, const size_t* ei, const size_t* ej, const double* ew,
+                         size_t m, const double* schedule_a, const double* schedule_b, size_t steps, size_t chi,
+                         int8_t* out_s, double* out_entropy) {
+    if (!out_s) {
+        set_err("out_s is NULL");
+        return std::nan("");
+    }
+    tessera_qa_problem p{n, h, m, ei, ej, ew, steps, schedule_a, schedule_b};
+    tessera_qa_config c;
+    tessera_qa_config_init(&c);
+    c.dt = 0.1;  // cuda/src/ffi.cpp:28
+    c.chi = chi;
+    tessera_qa_result r;
+    std::memset(&r, 0, sizeof(r));
+    std::vector<int8_t> spins(n);
+    std::vector<double> ent(steps);
+    r.spins = spins.data();
+    r.entropy = steps ? ent.data() : nullptr;
+    const int rc = tessera_qa_anneal_ex(&p, &c, &r);
+    if (rc != 0) return std::nan("");
+    std::memcpy(out_s, spins.data(), n);
+    if (out_entropy && steps) std::memcpy(out_entropy, ent.data(), sizeof(double) * steps);
+    return r.energy;
+}
+
+int tessera_qa_svd(const double* a, size_t rows, size_t cols, double* s, double* u, double* vh) {
+    return guarded([&]() -> int {
+        if (!a || !s) throw ArgError("a or s is NULL");
+        if (rows == 0 || cols == 0 || rows > 2048 || cols > 2048) throw ArgError("matrix shape out of range");
+        const int R = (int)rows, N = (int)cols, k = std::min(R, N);
+        ProblemHost P;
+        P.n = 1;
+        P.h.assign(1, 0.0);
+        Config C;
+        C.chi = 1;
+        C.min_ld = std::max(R, N);
+        int dev = 0;
+        if (cudaGetDeviceCount(&dev) != cudaSuccess || dev == 0) throw CudaError("no CUDA device available");
+        Engine<double> eng(P, C);
+        std::vector<double2> cm((size_t)R * N);
+        for (int i = 0; i < R; ++i)
+            for (int j = 0; j < N; ++j) cm[(size_t)j * R + i] = make_double2(a[2 * ((size_t)i * N + j)], a[2 * ((size_t)i * N + j) + 1]);
+        std::vector<int> perm;
+        std::vector<double> sig;
+        std::vector<double2> Wc;
+        eng.svd_only(cm, R, N, perm, sig, Wc);
+        for (int t = 0; t < k; ++t) s[t] = sig[t];
+        if (u || vh) {
+            // U[:, t] = W[:, perm[t]] / sigma_t ; Vh[t, :] = U[:, t]^H A
+            std::vector<double2> U((size_t)R * k, make_double2(0, 0));
+            for (int t = 0; t < k; ++t) {
+                if (!(sig[t] > 1e-300)) continue;
+                for (int i = 0; i < R; ++i) {
+                    const double2 w = Wc[(size_t)perm[t] * R + i];
+                    U[(size_t)i * k + t] = make_double2(w.x / sig[t], w.y / sig[t]);
+                }
+            }
+            if (u) std::memcpy(u, U.data(), sizeof(double2) * U.size());
+            if (vh) {
+                for (int t = 0; t < k; ++t)
+                    for (int j = 0; j < N; ++j) {
+                        double re = 0, im = 0;
+                        if (sig[t] > 1e-300)
+                            for (int i = 0; i < R; ++i) {
+                                const double2 x = U[(size_t)i * k + t];
+                                const double ar = a[2 * ((size_t)i * N + j)], ai = a[2 * ((size_t)i * N + j) + 1];
+                                re += x.x * ar + x.y * ai;
+                                im += x.x * ai - x.y * ar;
+                            }
+                        vh[2 * ((size_t)t * N + j)] = re / (sig[t] > 1e-300 ? sig[t] : 1.0);
+                        vh[2 * ((size_t)t * N + j) + 1] = im / (sig[t] > 1e-300 ? sig[t] : 1.0);
+                    }
+            }
+        }
+        if (eng.status_) {
+            set_err("kernel status bits set: " + std::to_string(eng.status_));
+            return TESSERA_QA_ESTATUS;
+        }
+        return 0;
+    });
+}
+
+tessera_qa_session* tessera_qa_session_create(const tessera_qa_problem* problem, const tessera_qa_config* config) {
+    tessera_qa_session* out = nullptr;
+    const int rc = guarded([&]() -> int {
+        std::unique_ptr<tessera_qa_session> s(new tessera_qa_session);
+        s->P = validate_problem(problem);
+        s->C = validate_config(config);
+        s->eng = make_engine(s->P, s->C);
+        out = s.release();
+        return 0;
+    });
+    return rc == 0 ? out : nullptr;
+}
+
+int tessera_qa_session_randomize(tessera_qa_session* s, uint64_t seed) {
+    return guarded([&]() -> int {
+        if (!s) throw ArgError("session is NULL");
+        s->eng->randomize(seed);
+        return 0;
+    });
+}
+
+int tessera_qa_session_run(tessera_qa_session* s, size_t step_begin, size_t nsteps) {
+    return guarded([&]() -> int {
+        if (!s) throw ArgError("session is NULL");
+        s->eng->run((int)step_begin, (int)(step_begin + nsteps));
+        return 0;
+    });
+}
+
+void* tessera_qa_session_stream(tessera_qa_session* s) { return s ? (void*)s->eng->stream() : nullptr; }
+
+int tessera_qa_session_sync(tessera_qa_session* s, tessera_qa_result* result) {
+    return guarded([&]() -> int {
+        if (!s) throw ArgError("session is NULL");
+        tessera_qa_result r;
+        std::memset(&r, 0, sizeof(r));
+        s->eng->sync_stats(&r);
+        if (result) {
+            result->max_trunc = r.max_trunc;
+            result->two_site_updates = r.two_site_updates;
+            result->status = r.status;
+            result->max_sweeps = r.max_sweeps;
+            result->max_bond = r.max_bond;
+            result->device_ms = r.device_ms;
+        }
+        return 0;
+    });
+}
+
+int tessera_qa_session_observe(tessera_qa_session* s, tessera_qa_result* result) {
+    return guarded([&]() -> int {
+        if (!s || !result) throw ArgError("session or result is NULL");
+        s->eng->sync_stats(result);
+        s->eng->observe(result);
+        return 0;
+    });
+}
+
+int tessera_qa_session_save(tessera_qa_session* s, void* buf, size_t bytes) {
+    return guarded([&]() -> int {
+        if (!s) throw ArgError("session is NULL");
+        s->eng->save(buf, bytes, 0);
+        return 0;
+    });
+}
+
+int tessera_qa_session_load(tessera_qa_session* s, const void* buf, size_t bytes) {
+    return guarded([&]() -> int {
+        if (!s) throw ArgError("session is NULL");
+        s->eng->load(buf, bytes);
+        return 0;
+    });
+}
+
+void tessera_qa_session_destroy(tessera_qa_session* s) { delete s; }
+
+}  // extern "C"

@@ -1,0 +1,119 @@
+// engine.cuh -- device-side views of the MPS state and launch declarations.
+//
+// HBM layout (one instance):
+//   sites   : n site tensors, each a fixed-capacity slab of 2*cap*cap complex elements.
+//             Site i element (a, s, b) sits at sites[i*site_stride + (a*2 + s)*cap + b],
+//             the reference's (a*2+s)*Dr+b order (cuda/include/mps.hpp:27-35) with the
+//             row stride fixed at the capacity, so site i is the row-major matrix
+//             [(a,s), b] with leading dimension cap.
+//   dims    : n+1 ints, bond dimensions; dims[0] = dims[n] = 1; site i is
+//             (dims[i], 2, dims[i+1]).  Kernels read dims on the device, so the host
+//             never waits for a truncation result.
+//   theta/W : (2cap) x (2cap) column-major complex workspaces; theta[row + col*ld] with
+//             row = (a, s1) = 2a + s1, col = (s2, b) = s2*Dr + b (cuda/src/mps.cpp:49).
+#pragma once
+#include "common.cuh"
+
+namespace tq {
+
+template <typename T>
+struct MpsView {
+    cplx_t<T>* sites;
+    int* dims;
+    int n;
+    int cap;
+    long long site_stride;
+    __device__ __forceinline__ cplx_t<T>* site(int i) const { return sites + (long long)i * site_stride; }
+};
+
+// A two-site gate: kind 0 = SWAP, 1 = exp(-i theta Z Z) with theta = -B(step)*w[edge]*sub,
+// 2 = a general 4x4 given in `g` (row-major, basis |s_i s_{i+1}>).
+struct GateOp {
+    int bond;
+    int kind;
+    int edge;
+    int pad;
+};
+enum : int { GATE_SWAP = 0, GATE_ZZ = 1, GATE_GENERAL = 2 };
+
+struct ScheduleView {
+    const double* h;    // n longitudinal fields
+    const double* w;    // m couplings
+    const double* sa;   // steps, transverse weight A(s_k)
+    const double* sb;   // steps, problem weight B(s_k)
+    const int* step;    // device step counter (index into sa/sb)
+    double dt;          // Trotter step
+    double sub;         // dt / zz_substeps
+};
+
+struct RunStats {
+    double max_trunc;       // max discarded weight ratio over the run
+    long long updates;      // two-site updates performed
+    int max_sweeps;         // most Jacobi sweeps any update needed
+    int status;             // ST_* bits
+    int max_bond;           // largest bond dimension seen
+    int pad;
+};
+
+// Per-update SVD workspace.
+template <typename T>
+struct SvdWork {
+    cplx_t<T>* theta;   // gated theta, column-major, ld
+    cplx_t<T>* W;       // Jacobi working copy (theta J), column-major, ld
+    int ld;
+    double* sig2;       // per-column squared norms [2cap]
+    double* sig;        // sorted kept singular values [2cap]
+    int* perm;          // sorted column order [2cap]
+    int* counters;      // per-sweep rotation counts [max_sweeps]
+    GridBar* bar;
+    RunStats* stats;
+};
+
+// ---- launchers (kernels.cu) ----
+template <typename T>
+void launch_single_site(const MpsView<T>& mps, const ScheduleView& sch, int dl_ub_max, cudaStream_t s);
+template <typename T>
+void launch_theta(const MpsView<T>& mps, const ScheduleView& sch, GateOp op, const double* gen_gate,
+                  SvdWork<T> wk, int dl_ub, int dr_ub, cudaStream_t s);
+// R, N > 0 run a standalone SVD of an explicit R x N matrix in wk.W (no truncation).
+template <typename T>
+int launch_svd(const MpsView<T>& mps, int bond, int chi, double tol, int max_sweeps, SvdWork<T> wk,
+               int rows_ub, int cols_ub, int block_w, cudaStream_t s, int R = 0, int N = 0);
+template <typename T>
+void launch_absorb(const MpsView<T>& mps, int bond, SvdWork<T> wk, int rows_ub, int cols_ub, int keep_ub,
+                   cudaStream_t s);
+
+// Environment transfer chain.  Each step maps env E (ket x bra, ld = cap) through one
+// site, optionally with Z inserted on that site's physical index:
+//   left : E'[b,b'] = sum_{a,a',s} E[a,a'] A(a,s,b) z_s conj(A(a',s,b'))
+//   right: E'[a,a'] = sum_{s,b,b'} A(a,s,b) E[b,b'] z_s conj(A(a',s,b'))
+struct ChainStep {
+    int site;
+    int zflag;
+    long long in_off;   // element offset of the input env in `envs`
+    long long out_off;  // element offset of the output env
+};
+template <typename T>
+void launch_chain(const MpsView<T>& mps, int right, const ChainStep* d_steps, int nsteps, cplx_t<T>* envs,
+                  cplx_t<T>* scratch, GridBar* bar, RunStats* stats, int d_ub, cudaStream_t s);
+template <typename T>
+void launch_entropy(const MpsView<T>& mps, const cplx_t<T>* r1, double* out_entropy, const int* step,
+                    cudaStream_t s);
+// values[j] = Re sum_{b,b'} X_j[b,b'] Y_j[b,b'] over the dims of bond bond_j
+struct PairDot {
+    long long x_off;
+    long long y_off;
+    int bond;
+    int pad;
+};
+template <typename T>
+void launch_pair_dots(const MpsView<T>& mps, const cplx_t<T>* envs, const PairDot* d_jobs, int njobs,
+                      double* out, cudaStream_t s);
+template <typename T>
+void launch_amplitude(const MpsView<T>& mps, const int8_t* spins, cplx_t<T>* scratch, double* out_amp2,
+                      cudaStream_t s);
+void launch_step_inc(int* step, cudaStream_t s);
+template <typename T>
+void launch_init_plus(const MpsView<T>& mps, cudaStream_t s);
+
+}  // namespace tq

@@ -1,0 +1,894 @@
+// kernels.cu -- sm_100a kernels of the MPS-TEBD anneal.
+//
+//   K5 k_single_site : all n single-site half-step gates exp(-i dt/2 (-A X - B h Z)) in one
+//                      launch, built in closed form cos(phi) I - i sin(phi) n.sigma
+//                      (replaces cuda/src/mps.cpp:313-322,344-353 + linalg.cpp:174-197).
+//   K1 k_theta       : theta = G . (A_i A_{i+1}) -- the bond contraction as a tiled GEMM
+//                      whose register tile holds whole (s1,s2) quads, so the 4x4 gate is an
+//                      epilogue (cuda/src/mps.cpp:46-70).
+//   K2 k_svd         : cooperative one-sided (Hestenes) Jacobi on theta's columns, block
+//                      tournament ordering, column pairs reduced with warp shuffles;
+//                      ends with the sigma sort, keep rule and discarded weight (K3)
+//                      (replaces cuda/src/linalg.cpp:7-172 and mps.cpp:76-85).
+//   K4 k_absorb_*    : A <- U[:, :keep], C <- U[:, :keep]^dagger theta (= S Vh[:keep])
+//                      (cuda/src/mps.cpp:87-99).
+//   K6 k_chain       : environment transfers (right env for the qubit-0 entropy, left and
+//                      right envs and Z insertions for the final observables), O(n chi^3).
+//   K7 k_pair_dots, k_amplitude, k_entropy : closing contractions, in FP64.
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+#include "engine.cuh"
+
+namespace tq {
+
+#define TQ_CHECK(x)                                                                            \
+    do {                                                                                       \
+        cudaError_t e_ = (x);                                                                  \
+        if (e_ != cudaSuccess)                                                                 \
+            throw std::runtime_error(std::string("CUDA: ") + cudaGetErrorString(e_) + " at " + \
+                                     __FILE__ + ":" + std::to_string(__LINE__));               \
+    } while (0)
+
+static int g_num_sms = 0;
+static int num_sms() {
+    if (!g_num_sms) {
+        int dev = 0;
+        TQ_CHECK(cudaGetDevice(&dev));
+        TQ_CHECK(cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    return g_num_sms;
+}
+
+// ------------------------------------------------------------------------------------
+// initial state |+>^n (cuda/src/mps.cpp:9-17)
+// ------------------------------------------------------------------------------------
+template <typename T>
+__global__ void k_init_plus(MpsView<T> mps) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i <= mps.n) mps.dims[i] = 1;
+    if (i < mps.n) {
+        const T a = (T)0.70710678118654752440;
+        cplx_t<T>* s = mps.site(i);
+        s[0] = mk<cplx_t<T>>(a, 0);          // (0, 0, 0)
+        s[mps.cap] = mk<cplx_t<T>>(a, 0);    // (0, 1, 0)
+    }
+}
+
+template <typename T>
+void launch_init_plus(const MpsView<T>& mps, cudaStream_t s) {
+    k_init_plus<T><<<(mps.n + 1 + 127) / 128, 128, 0, s>>>(mps);
+    TQ_CHECK(cudaGetLastError());
+}
+
+__global__ void k_step_inc(int* step) { *step += 1; }
+void launch_step_inc(int* step, cudaStream_t s) {
+    k_step_inc<<<1, 1, 0, s>>>(step);
+    TQ_CHECK(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------------------------
+// K5: single-site half step.  g = -A X - B h Z = nx X + nz Z; exp(-i (dt/2) g) =
+// cos(phi) I - i sin(phi) (nx X + nz Z)/r with r = |(nx, nz)|, phi = r dt/2.
+// ------------------------------------------------------------------------------------
+template <typename T>
+__global__ void k_single_site(MpsView<T> mps, ScheduleView sch) {
+    using V = cplx_t<T>;
+    const int i = blockIdx.y;
+    const int k = *sch.step;
+    const double A = sch.sa[k], B = sch.sb[k];
+    const double nx = -A, nz = -B * sch.h[i];
+    const double r = sqrt(nx * nx + nz * nz);
+    double c = 1.0, sn = 0.0;
+    if (r > 0) {
+        const double phi = 0.5 * sch.dt * r;
+        c = cos(phi);
+        sn = sin(phi) / r;
+    }
+    // U = [[c - i sn nz, -i sn nx], [-i sn nx, c + i sn nz]]
+    const V u00 = mk<V>((T)c, (T)(-sn * nz)), u01 = mk<V>((T)0, (T)(-sn * nx));
+    const V u11 = mk<V>((T)c, (T)(sn * nz));
+    const int dl = mps.dims[i], dr = mps.dims[i + 1];
+    V* S = mps.site(i);
+    const int tot = dl * dr;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += gridDim.x * blockDim.x) {
+        const int a = t / dr, b = t - a * dr;
+        V* p0 = S + (long long)(2 * a) * mps.cap + b;
+        V* p1 = p0 + mps.cap;
+        const V x0 = *p0, x1 = *p1;
+        V y0 = czero<V>(), y1 = czero<V>();
+        cfma(y0, u00, x0); cfma(y0, u01, x1);
+        cfma(y1, u01, x0); cfma(y1, u11, x1);
+        *p0 = y0;
+        *p1 = y1;
+    }
+}
+
+template <typename T>
+void launch_single_site(const MpsView<T>& mps, const ScheduleView& sch, int d2_ub_max, cudaStream_t s) {
+    int bx = (d2_ub_max + 255) / 256;
+    if (bx < 1) bx = 1;
+    if (bx > 64) bx = 64;
+    dim3 grid(bx, mps.n);
+    k_single_site<T><<<grid, 256, 0, s>>>(mps, sch);
+    TQ_CHECK(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------------------------
+// K1: theta contraction with the gate as an epilogue.
+// T_{s1 s2}[a, b] = sum_c A[(2a+s1), c] C[c, (s2, b)]; out[(2a+r1), (r2*Dr+b)] =
+// sum_{s1 s2} G[r1 r2][s1 s2] T_{s1 s2}[a, b].  A CTA owns 32 a x 32 b quads; thread
+// (tx, ty) owns a in {tx, tx+16}, b in {ty, ty+16}, i.e. 16 complex accumulators.
+// ------------------------------------------------------------------------------------
+constexpr int TH_KC = 8;
+
+template <typename V>
+__device__ __forceinline__ void gate_of(const GateOp& op, const ScheduleView& sch, const double* gen, V g[16]) {
+    using T = decltype(V::x);
+    for (int q = 0; q < 16; ++q) g[q] = czero<V>();
+    if (op.kind == GATE_SWAP) {
+        g[0] = mk<V>(1, 0); g[1 * 4 + 2] = mk<V>(1, 0); g[2 * 4 + 1] = mk<V>(1, 0); g[15] = mk<V>(1, 0);
+    } else if (op.kind == GATE_ZZ) {
+        const double th = -sch.sb[*sch.step] * sch.w[op.edge] * sch.sub;
+        const double c = cos(th), s = sin(th);
+        g[0] = mk<V>((T)c, (T)(-s)); g[15] = g[0];       // exp(-i th) on |00>, |11>
+        g[5] = mk<V>((T)c, (T)s); g[10] = g[5];          // exp(+i th) on |01>, |10>
+    } else {
+        for (int q = 0; q < 16; ++q) g[q] = mk<V>((T)gen[2 * q], (T)gen[2 * q + 1]);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_theta(MpsView<T> mps, ScheduleView sch, GateOp op, const double* gen,
+                                               SvdWork<T> wk) {
+    using V = cplx_t<T>;
+    __shared__ V As[TH_KC][2][32];
+    __shared__ V Cs[TH_KC][2][32];
+    const int i = op.bond;
+    const int dl = mps.dims[i], mid = mps.dims[i + 1], dr = mps.dims[i + 2];
+    const int a0 = blockIdx.x * 32, b0 = blockIdx.y * 32;
+    if (a0 >= dl || b0 >= dr) return;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const V* A = mps.site(i);
+    const V* Cm = mps.site(i + 1);
+    const int cap = mps.cap;
+    V acc[2][2][2][2];  // [ia][ib][s1][s2]
+#pragma unroll
+    for (int x = 0; x < 16; ++x) (&acc[0][0][0][0])[x] = czero<V>();
+    for (int c0 = 0; c0 < mid; c0 += TH_KC) {
+        // A tile: 64 rows (a, s1) x KC; C tile: KC x (s2, 32 b)
+        for (int e = tid; e < 64 * TH_KC; e += 256) {
+            const int kk = e % TH_KC, rr = e / TH_KC;
+            const int a = a0 + (rr >> 1), s1 = rr & 1, c = c0 + kk;
+            As[kk][s1][rr >> 1] = (a < dl && c < mid) ? A[(long long)(2 * a + s1) * cap + c] : czero<V>();
+        }
+        for (int e = tid; e < 64 * TH_KC; e += 256) {
+            const int bb = e & 31, rest = e >> 5;
+            const int kk = rest >> 1, s2 = rest & 1, c = c0 + kk, b = b0 + bb;
+            Cs[kk][s2][bb] = (b < dr && c < mid) ? Cm[(long long)(2 * c + s2) * cap + b] : czero<V>();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < TH_KC; ++kk) {
+            V av[2][2], cv[2][2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u)
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    av[u][s] = As[kk][s][tx + 16 * u];
+                    cv[u][s] = Cs[kk][s][ty + 16 * u];
+                }
+#pragma unroll
+            for (int ia = 0; ia < 2; ++ia)
+#pragma unroll
+                for (int ib = 0; ib < 2; ++ib)
+#pragma unroll
+                    for (int s1 = 0; s1 < 2; ++s1)
+#pragma unroll
+                        for (int s2 = 0; s2 < 2; ++s2) cfma(acc[ia][ib][s1][s2], av[ia][s1], cv[ib][s2]);
+        }
+        __syncthreads();
+    }
+    V g[16];
+    gate_of(op, sch, gen, g);
+    const int ld = wk.ld;
+#pragma unroll
+    for (int ia = 0; ia < 2; ++ia)
+#pragma unroll
+        for (int ib = 0; ib < 2; ++ib) {
+            const int a = a0 + tx + 16 * ia, b = b0 + ty + 16 * ib;
+            if (a >= dl || b >= dr) continue;
+#pragma unroll
+            for (int r1 = 0; r1 < 2; ++r1)
+#pragma unroll
+                for (int r2 = 0; r2 < 2; ++r2) {
+                    V o = czero<V>();
+#pragma unroll
+                    for (int s1 = 0; s1 < 2; ++s1)
+#pragma unroll
+                        for (int s2 = 0; s2 < 2; ++s2) cfma(o, g[(r1 * 2 + r2) * 4 + s1 * 2 + s2], acc[ia][ib][s1][s2]);
+                    const long long idx = (long long)(2 * a + r1) + (long long)(r2 * dr + b) * ld;
+                    wk.theta[idx] = o;
+                    wk.W[idx] = o;
+                }
+        }
+}
+
+template <typename T>
+void launch_theta(const MpsView<T>& mps, const ScheduleView& sch, GateOp op, const double* gen_gate,
+                  SvdWork<T> wk, int dl_ub, int dr_ub, cudaStream_t s) {
+    dim3 grid((dl_ub + 31) / 32, (dr_ub + 31) / 32);
+    k_theta<T><<<grid, 256, 0, s>>>(mps, sch, op, gen_gate, wk);
+    TQ_CHECK(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------------------------
+// K2 + K3: cooperative one-sided Jacobi SVD of W (R x N, column-major).
+//
+// Columns are cut into blocks of BW; a round-robin tournament over the P (even) blocks
+// gives P-1 rounds per sweep, each with P/2 disjoint block pairs, one pair per CTA at a
+// time.  A CTA stages its 2*BW columns in shared memory and, on round 0 of a sweep,
+// first rotates the pairs inside each block; then it rotates the BW*BW cross pairs in BW
+// inner rounds of BW disjoint pairs.  Each pair (p, q) is owned by G = 256/BW threads:
+// alpha = |w_p|^2, beta = |w_q|^2, gamma = w_p^dagger w_q are reduced with warp
+// shuffles (and shared memory across the group's warps) in FP64, and the pair is
+// rotated when |gamma| > tol sqrt(alpha beta):
+//   zeta = (beta - alpha) / (2|gamma|), t = sign(zeta)/(|zeta| + sqrt(1 + zeta^2)),
+//   c = 1/sqrt(1+t^2), s = c t, e = gamma/|gamma|,
+//   w_p <- c w_p - s conj(e) w_q,   w_q <- s e w_p + c w_q.
+// A sweep with no rotation ends the iteration.  Column norms then give sigma; CTA 0
+// sorts them (bitonic, descending), applies the keep rule of cuda/src/mps.cpp:76-85
+// (keep = min(chi, k), then drop trailing sigma < 1e-14) and records the discarded
+// weight ratio.
+// ------------------------------------------------------------------------------------
+struct SvdParams {
+    int bond;
+    int R, N;          // > 0: explicit matrix shape (standalone SVD); else 2*dims[bond], 2*dims[bond+2]
+    int no_trunc;      // 1: keep all min(R, N) values, leave dims and run statistics alone
+    int chi;
+    double tol;
+    double tiny;       // columns with |w|^2 below this are never rotated
+    int max_sweeps;
+    int rows_cap;      // shared-memory column length
+};
+
+template <int G>
+__device__ __forceinline__ void group_reduce4(double v[4], double* red, int tid) {
+    // G threads per group; groups are aligned to G.
+    if (G <= 32) {
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) v[q] = warp_sum(v[q]);
+        const int warp = tid >> 5, lane = tid & 31;
+        if (lane == 0)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) red[warp * 4 + q] = v[q];
+        __syncthreads();
+        constexpr int WG = G / 32;
+        const int w0 = (tid / G) * WG;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            double s = 0.0;
+#pragma unroll
+            for (int w = 0; w < WG; ++w) s += red[(w0 + w) * 4 + q];
+            v[q] = s;
+        }
+    }
+}
+
+// Rotate local columns p, q (shared memory) of a group; returns 1 if rotated.
+template <typename T, int G>
+__device__ __forceinline__ int rotate_pair(cplx_t<T>* cp, cplx_t<T>* cq, bool valid, int R, double tol,
+                                           double tiny, double* red, int tid) {
+    using V = cplx_t<T>;
+    const int lg = tid % G;
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    if (valid) {
+        for (int r = lg; r < R; r += G) {
+            const V x = cp[r], y = cq[r];
+            v[0] += (double)x.x * x.x + (double)x.y * x.y;
+            v[1] += (double)y.x * y.x + (double)y.y * y.y;
+            v[2] += (double)x.x * y.x + (double)x.y * y.y;   // Re conj(x) y
+            v[3] += (double)x.x * y.y - (double)x.y * y.x;   // Im conj(x) y
+        }
+    }
+    group_reduce4<G>(v, red, tid);
+    if (!valid) return 0;
+    const double al = v[0], be = v[1];
+    const double g = sqrt(v[2] * v[2] + v[3] * v[3]);
+    if (!(al > tiny && be > tiny && g > tol * sqrt(al * be))) return 0;
+    const double zeta = (be - al) / (2.0 * g);
+    const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+    const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
+    const T er = (T)(v[2] / g), ei = (T)(v[3] / g);
+    const T cc = (T)c, ss = (T)s;
+    for (int r = lg; r < R; r += G) {
+        const V x = cp[r], y = cq[r];
+        // s conj(e) y and s e x
+        const T ey_re = er * y.x + ei * y.y, ey_im = er * y.y - ei * y.x;
+        const T ex_re = er * x.x - ei * x.y, ex_im = er * x.y + ei * x.x;
+        cp[r] = mk<V>(cc * x.x - ss * ey_re, cc * x.y - ss * ey_im);
+        cq[r] = mk<V>(ss * ex_re + cc * y.x, ss * ex_im + cc * y.y);
+    }
+    return 1;
+}
+
+__device__ __forceinline__ void tournament(int P, int r, int pr, int& I, int& J) {
+    const int Q = P - 1;
+    if (pr == 0) {
+        I = Q;
+        J = r;
+    } else {
+        I = (r + pr) % Q;
+        J = (r - pr + Q) % Q;
+    }
+}
+
+template <typename T, int BW>
+__global__ void __launch_bounds__(256) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdParams pp) {
+    using V = cplx_t<T>;
+    constexpr int G = 256 / BW;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    V* col = reinterpret_cast<V*>(smraw);  // [2*BW][rows_cap]
+    __shared__ double red[32];             // [8 warps][4]
+    __shared__ int s_rot;
+    const int tid = threadIdx.x;
+    const int R = pp.R > 0 ? pp.R : 2 * mps.dims[pp.bond];
+    const int N = pp.N > 0 ? pp.N : 2 * mps.dims[pp.bond + 2];
+    const int ld = wk.ld;
+    V* W = wk.W;
+    const int nb = (N + BW - 1) / BW;
+    const int P = nb + (nb & 1);
+    const unsigned int nblk = gridDim.x;
+    int* status = &wk.stats->status;
+    if (R > pp.rows_cap) {  // host sizing bug guard: never index past shared memory
+        if (blockIdx.x == 0 && tid == 0) atomicOr(status, ST_BAD_DIMS);
+        return;
+    }
+    const int grp = tid / G;
+    int sweep = 0;
+    bool converged = false;
+    for (; sweep < pp.max_sweeps; ++sweep) {
+        for (int r = 0; r < P - 1; ++r) {
+            for (int pr = blockIdx.x; pr < P / 2; pr += gridDim.x) {
+                int I, J;
+                tournament(P, r, pr, I, J);
+                // stage columns: local c < BW -> block I, c >= BW -> block J
+                for (int e = tid; e < 2 * BW * R; e += 256) {
+                    const int c = e / R, row = e - c * R;
+                    const int gc = (c < BW) ? I * BW + c : J * BW + (c - BW);
+                    if (gc < N) col[c * pp.rows_cap + row] = W[(long long)gc * ld + row];
+                }
+                if (tid == 0) s_rot = 0;
+                __syncthreads();
+                int rot = 0;
+                if constexpr (BW >= 2) if (r == 0) {
+                    // intra-block pairs: circle method over BW columns, both blocks at once
+                    const int half = BW / 2;
+                    const int blk = grp < half ? 0 : 1;
+                    const int ip = grp < half ? grp : grp - half;
+                    for (int t = 0; t < BW - 1; ++t) {
+                        int x, y;
+                        if (ip == 0) { x = BW - 1; y = t; }
+                        else { x = (t + ip) % (BW - 1); y = (t - ip + (BW - 1)) % (BW - 1); }
+                        const int base = blk ? J * BW : I * BW;
+                        const bool ok = (base + x < N) && (base + y < N);
+                        rot += rotate_pair<T, G>(col + (blk * BW + x) * pp.rows_cap, col + (blk * BW + y) * pp.rows_cap,
+                                                 ok, R, pp.tol, pp.tiny, red, tid);
+                        __syncthreads();
+                    }
+                }
+                for (int t = 0; t < BW; ++t) {
+                    const int p = grp, q = (grp + t) % BW;
+                    const bool ok = (I * BW + p < N) && (J * BW + q < N);
+                    rot += rotate_pair<T, G>(col + p * pp.rows_cap, col + (BW + q) * pp.rows_cap, ok, R, pp.tol,
+                                             pp.tiny, red, tid);
+                    __syncthreads();
+                }
+                if (rot && (tid % G) == 0) atomicAdd(&s_rot, rot);
+                __syncthreads();
+                for (int e = tid; e < 2 * BW * R; e += 256) {
+                    const int c = e / R, row = e - c * R;
+                    const int gc = (c < BW) ? I * BW + c : J * BW + (c - BW);
+                    if (gc < N) W[(long long)gc * ld + row] = col[c * pp.rows_cap + row];
+                }
+                if (tid == 0 && s_rot) atomicAdd(&wk.counters[sweep], s_rot);
+                __syncthreads();
+            }
+            if (!grid_sync(wk.bar, status, nblk)) return;
+        }
+        const int done = *(volatile int*)&wk.counters[sweep];
+        if (done == 0) {
+            converged = true;
+            ++sweep;
+            break;
+        }
+    }
+    // column norms -> sig2 (FP64)
+    {
+        const int warp = tid >> 5, lane = tid & 31;
+        for (int j = blockIdx.x * 8 + warp; j < N; j += gridDim.x * 8) {
+            double s = 0.0;
+            const V* w = W + (long long)j * ld;
+            for (int row = lane; row < R; row += 32) s += (double)w[row].x * w[row].x + (double)w[row].y * w[row].y;
+            s = warp_sum(s);
+            if (lane == 0) wk.sig2[j] = s;
+        }
+    }
+    if (!grid_sync(wk.bar, status, nblk)) return;
+    if (blockIdx.x != 0) return;
+    // ---- K3: sort + keep rule + discarded weight (CTA 0) ----
+    double* key = reinterpret_cast<double*>(smraw);
+    int* idx = reinterpret_cast<int*>(key + 4096);
+    int P2 = 1;
+    while (P2 < N) P2 <<= 1;
+    for (int e = tid; e < P2; e += 256) {
+        key[e] = e < N ? wk.sig2[e] : -1.0;
+        idx[e] = e;
+    }
+    __syncthreads();
+    for (int k = 2; k <= P2; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int e = tid; e < P2; e += 256) {
+                const int o = e ^ j;
+                if (o > e) {
+                    const bool desc = ((e & k) == 0);
+                    const double ke = key[e], ko = key[o];
+                    const int ie = idx[e], io = idx[o];
+                    // "e before o" in descending order with ascending-index tie break
+                    const bool e_first = (ke > ko) || (ke == ko && ie < io);
+                    if (desc ? !e_first : e_first) {
+                        key[e] = ko; key[o] = ke; idx[e] = io; idx[o] = ie;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    const int kk = R < N ? R : N;
+    const int keep0 = pp.chi < kk ? pp.chi : kk;
+    double tot = 0.0, big = 0.0;
+    for (int e = tid; e < kk; e += 256) {
+        const double v = key[e] > 0 ? key[e] : 0.0;
+        tot += v;
+        if (e < keep0 && sqrt(v) >= 1e-14) big += 1.0;
+    }
+    tot = warp_sum(tot);
+    big = warp_sum(big);
+    if ((tid & 31) == 0) { red[(tid >> 5) * 4] = tot; red[(tid >> 5) * 4 + 1] = big; }
+    __syncthreads();
+    __shared__ int s_keep;
+    __shared__ double s_tot;
+    if (tid == 0) {
+        double t2 = 0.0, b2 = 0.0;
+        for (int w = 0; w < 8; ++w) { t2 += red[w * 4]; b2 += red[w * 4 + 1]; }
+        int keep = pp.no_trunc ? kk : (int)b2;
+        if (keep < 1) keep = 1;
+        s_keep = keep;
+        s_tot = t2;
+    }
+    __syncthreads();
+    const int keep = s_keep;
+    double disc = 0.0;
+    for (int e = keep + tid; e < kk; e += 256) disc += key[e] > 0 ? key[e] : 0.0;
+    disc = warp_sum(disc);
+    __syncthreads();
+    if ((tid & 31) == 0) red[(tid >> 5) * 4 + 2] = disc;
+    for (int e = tid; e < keep; e += 256) {
+        wk.perm[e] = idx[e];
+        wk.sig[e] = sqrt(key[e] > 0 ? key[e] : 0.0);
+    }
+    __syncthreads();
+    if (tid == 0 && !pp.no_trunc) {
+        double d2 = 0.0;
+        for (int w = 0; w < 8; ++w) d2 += red[w * 4 + 2];
+        RunStats* st = wk.stats;
+        if (s_tot > 0) {
+            const double ratio = d2 / s_tot;
+            if (ratio > st->max_trunc) st->max_trunc = ratio;
+        }
+        if (!isfinite(s_tot)) st->status |= ST_NONFINITE;
+        if (!converged) st->status |= ST_JACOBI_NOT_CONVERGED;
+        if (sweep > st->max_sweeps) st->max_sweeps = sweep;
+        if (keep > st->max_bond) st->max_bond = keep;
+        st->updates += 1;
+        mps.dims[pp.bond + 1] = keep;
+    }
+}
+
+template <typename T, int BW>
+static int svd_launch_bw(const MpsView<T>& mps, const SvdParams& pp, SvdWork<T> wk, int cols_ub,
+                         cudaStream_t s) {
+    using V = cplx_t<T>;
+    size_t smem = sizeof(V) * 2 * BW * (size_t)pp.rows_cap;
+    const size_t sort_smem = 4096 * (sizeof(double) + sizeof(int));
+    if (smem < sort_smem) smem = sort_smem;
+    auto fn = k_svd<T, BW>;
+    TQ_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    TQ_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, smem));
+    if (per_sm < 1) throw std::runtime_error("k_svd does not fit on an SM");
+    const int nb = (cols_ub + BW - 1) / BW;
+    const int pairs = (nb + (nb & 1)) / 2;
+    int grid = pairs < 1 ? 1 : pairs;
+    const int maxg = per_sm * num_sms();
+    if (grid > maxg) grid = maxg;
+    MpsView<T> m = mps;
+    SvdParams p = pp;
+    void* args[] = {&m, &wk, &p};
+    TQ_CHECK(cudaLaunchCooperativeKernel((const void*)fn, dim3(grid), dim3(256), args, smem, s));
+    return grid;
+}
+
+template <typename T>
+int launch_svd(const MpsView<T>& mps, int bond, int chi, double tol, int max_sweeps, SvdWork<T> wk,
+               int rows_ub, int cols_ub, int block_w, cudaStream_t s, int R, int N) {
+    SvdParams pp;
+    pp.bond = bond;
+    pp.R = R;
+    pp.N = N;
+    pp.no_trunc = R > 0 ? 1 : 0;
+    pp.chi = chi;
+    pp.tol = tol;
+    pp.tiny = sizeof(T) == 8 ? 1e-200 : 1e-60;
+    pp.max_sweeps = max_sweeps;
+    pp.rows_cap = (rows_ub + 7) & ~7;
+    if (pp.rows_cap < 8) pp.rows_cap = 8;
+    TQ_CHECK(cudaMemsetAsync(wk.counters, 0, sizeof(int) * max_sweeps, s));
+    switch (block_w) {
+        case 1: return svd_launch_bw<T, 1>(mps, pp, wk, cols_ub, s);
+        case 2: return svd_launch_bw<T, 2>(mps, pp, wk, cols_ub, s);
+        case 4: return svd_launch_bw<T, 4>(mps, pp, wk, cols_ub, s);
+        case 8: return svd_launch_bw<T, 8>(mps, pp, wk, cols_ub, s);
+        case 16: return svd_launch_bw<T, 16>(mps, pp, wk, cols_ub, s);
+        default: throw std::runtime_error("unsupported Jacobi block width");
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// K4: absorption.  A_new(a, s1, k) = W[(2a+s1), perm[k]] / sigma_k ;
+// C_new(k, s2, b) = (1/sigma_k) sum_row conj(W[row, perm[k]]) theta[row, s2*Dr + b].
+// ------------------------------------------------------------------------------------
+template <typename T>
+__global__ void k_absorb_u(MpsView<T> mps, int bond, SvdWork<T> wk) {
+    using V = cplx_t<T>;
+    const int R = 2 * mps.dims[bond];
+    const int keep = mps.dims[bond + 1];
+    const int k = blockIdx.x * 32 + threadIdx.x;
+    const int row = blockIdx.y * 8 + threadIdx.y;
+    if (k >= keep || row >= R) return;
+    const double inv = 1.0 / wk.sig[k];
+    const V w = wk.W[(long long)wk.perm[k] * wk.ld + row];
+    mps.site(bond)[(long long)row * mps.cap + k] = mk<V>((T)(w.x * inv), (T)(w.y * inv));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_absorb_c(MpsView<T> mps, int bond, SvdWork<T> wk) {
+    using V = cplx_t<T>;
+    constexpr int KC = 8;
+    __shared__ V Us[KC][32];
+    __shared__ V Ts[KC][32];
+    __shared__ int pk[32];
+    const int R = 2 * mps.dims[bond];
+    const int keep = mps.dims[bond + 1];
+    const int dr = mps.dims[bond + 2];
+    const int N = 2 * dr;
+    const int k0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    if (k0 >= keep || c0 >= N) return;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    if (tid < 32) pk[tid] = (k0 + tid < keep) ? wk.perm[k0 + tid] : -1;
+    __syncthreads();
+    const int ld = wk.ld;
+    V acc[2][2];
+    for (int q = 0; q < 4; ++q) (&acc[0][0])[q] = czero<V>();
+    for (int r0 = 0; r0 < R; r0 += KC) {
+        {
+            const int kk = tid % KC, q = tid / KC;  // 256 = 8 x 32
+            const int row = r0 + kk;
+            const int pc = pk[q];
+            V u = czero<V>();
+            if (pc >= 0 && row < R) { u = wk.W[(long long)pc * ld + row]; u.y = -u.y; }
+            Us[kk][q] = u;
+            const int col = c0 + q;
+            Ts[kk][q] = (col < N && row < R) ? wk.theta[(long long)col * ld + row] : czero<V>();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < KC; ++kk) {
+            const V u0 = Us[kk][ty], u1 = Us[kk][ty + 16];
+            const V t0 = Ts[kk][tx], t1 = Ts[kk][tx + 16];
+            cfma(acc[0][0], u0, t0); cfma(acc[0][1], u0, t1);
+            cfma(acc[1][0], u1, t0); cfma(acc[1][1], u1, t1);
+        }
+        __syncthreads();
+    }
+    V* Cn = mps.site(bond + 1);
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int k = k0 + ty + 16 * i, col = c0 + tx + 16 * j;
+            if (k >= keep || col >= N) continue;
+            const int s2 = col >= dr ? 1 : 0, b = col - s2 * dr;
+            const double inv = 1.0 / wk.sig[k];
+            const V v = acc[i][j];
+            Cn[(long long)(2 * k + s2) * mps.cap + b] = mk<V>((T)(v.x * inv), (T)(v.y * inv));
+        }
+}
+
+template <typename T>
+void launch_absorb(const MpsView<T>& mps, int bond, SvdWork<T> wk, int rows_ub, int cols_ub, int keep_ub,
+                   cudaStream_t s) {
+    k_absorb_u<T><<<dim3((keep_ub + 31) / 32, (rows_ub + 7) / 8), dim3(32, 8), 0, s>>>(mps, bond, wk);
+    TQ_CHECK(cudaGetLastError());
+    k_absorb_c<T><<<dim3((cols_ub + 31) / 32, (keep_ub + 31) / 32), 256, 0, s>>>(mps, bond, wk);
+    TQ_CHECK(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------------------------
+// K6: environment transfer chain (cooperative; two GEMM phases per step).
+// ------------------------------------------------------------------------------------
+template <typename V, class LA, class LB, class ST>
+__device__ void gemm_phase(int M, int N, int K, LA la, LB lb, ST st, V (*As)[32], V (*Bs)[32]) {
+    constexpr int KC = 8;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int tm = (M + 31) / 32, tn = (N + 31) / 32;
+    for (int t = blockIdx.x; t < tm * tn; t += gridDim.x) {
+        const int i0 = (t / tn) * 32, j0 = (t % tn) * 32;
+        V acc[2][2];
+        for (int q = 0; q < 4; ++q) (&acc[0][0])[q] = czero<V>();
+        for (int k0 = 0; k0 < K; k0 += KC) {
+            {
+                const int kk = tid % KC, q = tid / KC;
+                const int k = k0 + kk;
+                As[kk][q] = (i0 + q < M && k < K) ? la(i0 + q, k) : czero<V>();
+                Bs[kk][q] = (j0 + q < N && k < K) ? lb(k, j0 + q) : czero<V>();
+            }
+            __syncthreads();
+#pragma unroll
+            for (int kk = 0; kk < KC; ++kk) {
+                const V a0 = As[kk][ty], a1 = As[kk][ty + 16];
+                const V b0 = Bs[kk][tx], b1 = Bs[kk][tx + 16];
+                cfma(acc[0][0], a0, b0); cfma(acc[0][1], a0, b1);
+                cfma(acc[1][0], a1, b0); cfma(acc[1][1], a1, b1);
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const int ii = i0 + ty + 16 * i, jj = j0 + tx + 16 * j;
+                if (ii < M && jj < N) st(ii, jj, acc[i][j]);
+            }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_chain(MpsView<T> mps, int right, const ChainStep* steps, int nsteps,
+                                               cplx_t<T>* envs, cplx_t<T>* X, GridBar* bar, RunStats* stats) {
+    using V = cplx_t<T>;
+    __shared__ V As[8][32];
+    __shared__ V Bs[8][32];
+    const int cap = mps.cap;
+    const int ldx = 2 * cap;
+    const unsigned int nblk = gridDim.x;
+    for (int q = 0; q < nsteps; ++q) {
+        const ChainStep cs = steps[q];
+        const int dl = mps.dims[cs.site], dr = mps.dims[cs.site + 1];
+        const V* A = mps.site(cs.site);
+        const V* E = envs + cs.in_off;
+        V* O = envs + cs.out_off;
+        const bool z = cs.zflag != 0;
+        if (!right) {
+            // Y[a', s*dr + b] = sum_a E[a, a'] A[(2a+s), b] z_s
+            gemm_phase<V>(dl, 2 * dr, dl,
+                [&](int i, int k) { return E[(long long)k * cap + i]; },
+                [&](int k, int j) {
+                    const int s = j >= dr ? 1 : 0, b = j - s * dr;
+                    V v = A[(long long)(2 * k + s) * cap + b];
+                    if (z && s) { v.x = -v.x; v.y = -v.y; }
+                    return v;
+                },
+                [&](int i, int j, V v) { X[(long long)i * ldx + j] = v; }, As, Bs);
+            if (!grid_sync(bar, &stats->status, nblk)) return;
+            // O[b, b'] = sum_{a', s} Y[a', s*dr + b] conj(A[(2a'+s), b'])
+            gemm_phase<V>(dr, dr, 2 * dl,
+                [&](int i, int k) { return X[(long long)(k >> 1) * ldx + (k & 1) * dr + i]; },
+                [&](int k, int j) { V v = A[(long long)k * cap + j]; v.y = -v.y; return v; },
+                [&](int i, int j, V v) { O[(long long)i * cap + j] = v; }, As, Bs);
+        } else {
+            // X[(2a+s), b'] = sum_b A[(2a+s), b] E[b, b'] z_s
+            gemm_phase<V>(2 * dl, dr, dr,
+                [&](int i, int k) {
+                    V v = A[(long long)i * cap + k];
+                    if (z && (i & 1)) { v.x = -v.x; v.y = -v.y; }
+                    return v;
+                },
+                [&](int k, int j) { return E[(long long)k * cap + j]; },
+                [&](int i, int j, V v) { X[(long long)i * ldx + j] = v; }, As, Bs);
+            if (!grid_sync(bar, &stats->status, nblk)) return;
+            // O[a, a'] = sum_{s, b'} X[(2a+s), b'] conj(A[(2a'+s), b'])   (k = s*dr + b')
+            gemm_phase<V>(dl, dl, 2 * dr,
+                [&](int i, int k) {
+                    const int s = k >= dr ? 1 : 0, b = k - s * dr;
+                    return X[(long long)(2 * i + s) * ldx + b];
+                },
+                [&](int k, int j) {
+                    const int s = k >= dr ? 1 : 0, b = k - s * dr;
+                    V v = A[(long long)(2 * j + s) * cap + b];
+                    v.y = -v.y;
+                    return v;
+                },
+                [&](int i, int j, V v) { O[(long long)i * cap + j] = v; }, As, Bs);
+        }
+        if (!grid_sync(bar, &stats->status, nblk)) return;
+    }
+}
+
+template <typename T>
+void launch_chain(const MpsView<T>& mps, int right, const ChainStep* d_steps, int nsteps, cplx_t<T>* envs,
+                  cplx_t<T>* scratch, GridBar* bar, RunStats* stats, int d_ub, cudaStream_t s) {
+    if (nsteps <= 0) return;
+    auto fn = k_chain<T>;
+    int per_sm = 0;
+    TQ_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0));
+    const int tiles = ((2 * d_ub + 31) / 32) * ((d_ub + 31) / 32);
+    int grid = tiles < 1 ? 1 : tiles;
+    const int maxg = per_sm * num_sms();
+    if (grid > maxg) grid = maxg;
+    MpsView<T> m = mps;
+    int r = right;
+    int ns = nsteps;
+    void* args[] = {&m, &r, (void*)&d_steps, &ns, &envs, &scratch, &bar, &stats};
+    TQ_CHECK(cudaLaunchCooperativeKernel((const void*)fn, dim3(grid), dim3(256), args, 0, s));
+}
+
+// rho_0[s, s'] = sum_{b, b'} A0[s, b] R1[b, b'] conj(A0[s', b']), entropy in bits of rho/tr
+// with eigenvalues clamped to [0, 1] and terms lambda <= 1e-12 dropped
+// (cuda/src/mps.cpp:218-291).
+template <typename T>
+__global__ void k_entropy(MpsView<T> mps, const cplx_t<T>* r1, double* out, const int* step) {
+    using V = cplx_t<T>;
+    __shared__ double red[8][8];
+    const int tid = threadIdx.x;
+    const int d = mps.dims[1];
+    const V* A = mps.site(0);
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // rho00, rho11 (re), rho01 (re, im)
+    for (int bp = tid; bp < d; bp += blockDim.x) {
+        double v0r = 0, v0i = 0, v1r = 0, v1i = 0;
+        for (int b = 0; b < d; ++b) {
+            const V rr = r1 ? r1[(long long)b * mps.cap + bp] : mk<V>(1, 0);
+            const V x0 = A[b], x1 = A[mps.cap + b];
+            v0r += (double)x0.x * rr.x - (double)x0.y * rr.y;
+            v0i += (double)x0.x * rr.y + (double)x0.y * rr.x;
+            v1r += (double)x1.x * rr.x - (double)x1.y * rr.y;
+            v1i += (double)x1.x * rr.y + (double)x1.y * rr.x;
+        }
+        const V y0 = A[bp], y1 = A[mps.cap + bp];
+        // v_s[bp] * conj(A0[s', bp])
+        acc[0] += v0r * y0.x + v0i * y0.y;
+        acc[1] += v1r * y1.x + v1i * y1.y;
+        acc[2] += v0r * y1.x + v0i * y1.y;
+        acc[3] += v0i * y1.x - v0r * y1.y;
+    }
+    for (int q = 0; q < 4; ++q) acc[q] = warp_sum(acc[q]);
+    if ((tid & 31) == 0)
+        for (int q = 0; q < 4; ++q) red[tid >> 5][q] = acc[q];
+    __syncthreads();
+    if (tid == 0) {
+        double r00 = 0, r11 = 0, r01r = 0, r01i = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            r00 += red[w][0]; r11 += red[w][1]; r01r += red[w][2]; r01i += red[w][3];
+        }
+        const double tr = r00 + r11;
+        double S = 0.0;
+        if (tr > 0) {
+            const double p = r00 / tr, q = r11 / tr;
+            const double off2 = (r01r * r01r + r01i * r01i) / (tr * tr);
+            const double mid = 0.5 * (p + q);
+            const double rad = sqrt(fmax(0.0, 0.25 * (p - q) * (p - q) + off2));
+            const double l1 = fmin(1.0, fmax(0.0, mid + rad)), l2 = fmin(1.0, fmax(0.0, mid - rad));
+            if (l1 > 1e-12) S -= l1 * log2(l1);
+            if (l2 > 1e-12) S -= l2 * log2(l2);
+        }
+        out[*step] = S;
+    }
+}
+
+template <typename T>
+void launch_entropy(const MpsView<T>& mps, const cplx_t<T>* r1, double* out_entropy, const int* step,
+                    cudaStream_t s) {
+    k_entropy<T><<<1, 256, 0, s>>>(mps, r1, out_entropy, step);
+    TQ_CHECK(cudaGetLastError());
+}
+
+template <typename T>
+__global__ void k_pair_dots(MpsView<T> mps, const cplx_t<T>* envs, const PairDot* jobs, double* out) {
+    using V = cplx_t<T>;
+    __shared__ double red[8];
+    const PairDot jb = jobs[blockIdx.x];
+    const int d = mps.dims[jb.bond];
+    const V* X = envs + jb.x_off;
+    const V* Y = envs + jb.y_off;
+    double acc = 0.0;
+    for (int e = threadIdx.x; e < d * d; e += blockDim.x) {
+        const int b = e / d, bp = e - b * d;
+        const V x = X[(long long)b * mps.cap + bp], y = Y[(long long)b * mps.cap + bp];
+        acc += (double)x.x * y.x - (double)x.y * y.y;
+    }
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+        out[blockIdx.x] = s;
+    }
+}
+
+template <typename T>
+void launch_pair_dots(const MpsView<T>& mps, const cplx_t<T>* envs, const PairDot* d_jobs, int njobs, double* out,
+                      cudaStream_t s) {
+    if (njobs <= 0) return;
+    k_pair_dots<T><<<njobs, 256, 0, s>>>(mps, envs, d_jobs, out);
+    TQ_CHECK(cudaGetLastError());
+}
+
+// |<x|psi>|^2 for one spin pattern (+1 <-> physical 0), cuda/src/mps.cpp:197-216.
+template <typename T>
+__global__ void k_amplitude(MpsView<T> mps, const int8_t* spins, cplx_t<T>* vbuf, double* out) {
+    using V = cplx_t<T>;
+    V* v = vbuf;
+    V* w = vbuf + mps.cap;
+    if (threadIdx.x == 0) v[0] = mk<V>(1, 0);
+    __syncthreads();
+    for (int i = 0; i < mps.n; ++i) {
+        const int dl = mps.dims[i], dr = mps.dims[i + 1];
+        const int s = spins[i] > 0 ? 0 : 1;
+        const V* A = mps.site(i);
+        for (int b = threadIdx.x; b < dr; b += blockDim.x) {
+            double re = 0, im = 0;
+            for (int a = 0; a < dl; ++a) {
+                const V x = v[a], y = A[(long long)(2 * a + s) * mps.cap + b];
+                re += (double)x.x * y.x - (double)x.y * y.y;
+                im += (double)x.x * y.y + (double)x.y * y.x;
+            }
+            w[b] = mk<V>((T)re, (T)im);
+        }
+        __syncthreads();
+        V* t = v; v = w; w = t;
+    }
+    if (threadIdx.x == 0) out[0] = (double)v[0].x * v[0].x + (double)v[0].y * v[0].y;
+}
+
+template <typename T>
+void launch_amplitude(const MpsView<T>& mps, const int8_t* spins, cplx_t<T>* scratch, double* out_amp2,
+                      cudaStream_t s) {
+    k_amplitude<T><<<1, 256, 0, s>>>(mps, spins, scratch, out_amp2);
+    TQ_CHECK(cudaGetLastError());
+}
+
+// explicit instantiations
+#define TQ_INST(T)                                                                                          \
+    template void launch_init_plus<T>(const MpsView<T>&, cudaStream_t);                                     \
+    template void launch_single_site<T>(const MpsView<T>&, const ScheduleView&, int, cudaStream_t);         \
+    template void launch_theta<T>(const MpsView<T>&, const ScheduleView&, GateOp, const double*, SvdWork<T>, \
+                                  int, int, cudaStream_t);                                                  \
+    template int launch_svd<T>(const MpsView<T>&, int, int, double, int, SvdWork<T>, int, int, int,         \
+                               cudaStream_t, int, int);                                                     \
+    template void launch_absorb<T>(const MpsView<T>&, int, SvdWork<T>, int, int, int, cudaStream_t);        \
+    template void launch_chain<T>(const MpsView<T>&, int, const ChainStep*, int, cplx_t<T>*, cplx_t<T>*,   \
+                                  GridBar*, RunStats*, int, cudaStream_t);                                  \
+    template void launch_entropy<T>(const MpsView<T>&, const cplx_t<T>*, double*, const int*, cudaStream_t); \
+    template void launch_pair_dots<T>(const MpsView<T>&, const cplx_t<T>*, const PairDot*, int, double*,    \
+                                      cudaStream_t);                                                        \
+    template void launch_amplitude<T>(const MpsView<T>&, const int8_t*, cplx_t<T>*, double*, cudaStream_t);
+TQ_INST(double)
+TQ_INST(float)
+
+}  // namespace tq

@@ -1,0 +1,229 @@
+"""Host-side interface of the anneal path, mirroring the reference's Rust caller.
+
+``quantum_anneal(model, sched, chi)`` is the counterpart of rust/src/ffi.rs:47-85: it
+splits the model's couplings into ei/ej/ew arrays, rejects schedules shorter than two
+steps with ``QaError.BadSchedule`` (rust/src/ffi.rs:49-51) and calls the legacy
+``tessera_qa_anneal`` symbol of libtessera_qa.so exactly as the Rust wrapper does
+(rust/src/ffi.rs:60-75).  ``anneal`` exposes the extended entry point (dt, precision,
+Jacobi controls, checkpoints, every result field).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+
+
+class QaError(enum.Enum):
+    """rust/src/ffi.rs:11-17 (EngineNotLinked cannot occur: the engine is always linked)."""
+
+    EngineNotLinked = "EngineNotLinked"
+    BadSchedule = "BadSchedule"
+
+
+class QaException(Exception):
+    def __init__(self, err: QaError):
+        super().__init__(err.value)
+        self.err = err
+
+
+@dataclass
+class Ising:
+    """Problem model of rust/src/ising.rs:11-32: fields h and couplings (i, j, w)."""
+
+    h: list
+    j: list  # [(i, k, w), ...]
+
+    @property
+    def n(self) -> int:
+        return len(self.h)
+
+    def energy(self, s) -> float:
+        e = 0.0
+        for (i, k, w) in self.j:
+            e -= w * s[i] * s[k]
+        for hi, si in zip(self.h, s):
+            e -= hi * si
+        return e
+
+
+@dataclass
+class Schedule:
+    """rust/src/schedule.rs:8-18."""
+
+    a: list
+    b: list
+
+    def steps(self) -> int:
+        return len(self.a)
+
+
+@dataclass
+class QaResult:
+    """rust/src/ffi.rs:39-43."""
+
+    spins: np.ndarray
+    energy: float
+    entropy: np.ndarray
+
+
+def _arr(x, dtype):
+    return np.ascontiguousarray(np.asarray(x, dtype=dtype))
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t) if a is not None and a.size else None
+
+
+def quantum_anneal(model: Ising, sched: Schedule, chi: int) -> QaResult:
+    steps = sched.steps()
+    if steps < 2:
+        raise QaException(QaError.BadSchedule)
+    L = _lib.load()
+    h = _arr(model.h, np.float64)
+    ei = _arr([t[0] for t in model.j], np.uint64)
+    ej = _arr([t[1] for t in model.j], np.uint64)
+    ew = _arr([t[2] for t in model.j], np.float64)
+    a = _arr(sched.a, np.float64)
+    b = _arr(sched.b, np.float64)
+    spins = np.zeros(model.n, np.int8)
+    entropy = np.zeros(steps, np.float64)
+    e = L.tessera_qa_anneal(_p(h, _lib.c_double_p), model.n, _p(ei, _lib.c_size_p), _p(ej, _lib.c_size_p),
+                            _p(ew, _lib.c_double_p), len(model.j), _p(a, _lib.c_double_p), _p(b, _lib.c_double_p),
+                            steps, chi, _p(spins, _lib.c_int8_p), _p(entropy, _lib.c_double_p))
+    if np.isnan(e):
+        raise _lib.EngineError(_lib.EINVAL, _lib.last_error())
+    return QaResult(spins, float(e), entropy)
+
+
+@dataclass
+class AnnealResult:
+    """All fields of tessera_qa_result (the reference's AnnealResult, cuda/include/mps.hpp:37-44, plus
+    run statistics)."""
+
+    spins: np.ndarray
+    energy: float
+    expected_energy: float
+    prob: float
+    max_trunc: float
+    norm2: float
+    entropy: np.ndarray
+    two_site_updates: int
+    status: int
+    max_sweeps: int
+    max_bond: int
+    device_ms: float
+    checkpoint: bytes | None = None
+    extra: dict = field(default_factory=dict)
+
+
+def problem_struct(h, ei, ej, ew, sa, sb):
+    """Build a tessera_qa_problem; returns (struct, keepalive arrays)."""
+    h = _arr(h, np.float64)
+    ei = _arr(ei, np.uint64)
+    ej = _arr(ej, np.uint64)
+    ew = _arr(ew, np.float64)
+    sa = _arr(sa, np.float64)
+    sb = _arr(sb, np.float64)
+    P = _lib.Problem(len(h), _p(h, _lib.c_double_p), len(ew), _p(ei, _lib.c_size_p), _p(ej, _lib.c_size_p),
+                     _p(ew, _lib.c_double_p), len(sa), _p(sa, _lib.c_double_p), _p(sb, _lib.c_double_p))
+    return P, (h, ei, ej, ew, sa, sb)
+
+
+def config_struct(dt=0.1, chi=32, precision="c128", zz_substeps=1, jacobi_tol=0.0, jacobi_max_sweeps=0,
+                  jacobi_block=0, device=-1, step_begin=0, step_end=0, initial_mps=None, skip_observables=False):
+    L = _lib.load()
+    c = _lib.Config()
+    L.tessera_qa_config_init(C.byref(c))
+    c.dt = dt
+    c.chi = chi
+    c.precision = _lib.TESSERA_QA_C64 if precision in ("c64", "complex64", 1) else _lib.TESSERA_QA_C128
+    c.zz_substeps = zz_substeps
+    c.jacobi_tol = jacobi_tol
+    c.jacobi_max_sweeps = jacobi_max_sweeps
+    c.jacobi_block = jacobi_block
+    c.device = device
+    c.step_begin = step_begin
+    c.step_end = step_end
+    keep = None
+    if initial_mps is not None:
+        keep = np.frombuffer(initial_mps, dtype=np.uint8).copy()
+        c.initial_mps = keep.ctypes.data
+    c.skip_observables = 1 if skip_observables else 0
+    return c, keep
+
+
+def anneal(h, ei, ej, ew, sa, sb, dt=0.1, chi=32, precision="c128", zz_substeps=1, want_checkpoint=False,
+           raise_on_status=True, **kw) -> AnnealResult:
+    """tessera_qa_anneal_ex: the MPS-TEBD anneal with every result field."""
+    L = _lib.load()
+    P, keep = problem_struct(h, ei, ej, ew, sa, sb)
+    c, keep2 = config_struct(dt=dt, chi=chi, precision=precision, zz_substeps=zz_substeps, **kw)
+    n = int(P.n)
+    k0 = int(c.step_begin)
+    k1 = int(c.step_end) if c.step_end else int(P.steps)
+    spins = np.zeros(n, np.int8)
+    ent = np.zeros(max(k1 - k0, 1), np.float64)
+    r = _lib.Result()
+    r.spins = _p(spins, _lib.c_int8_p)
+    r.entropy = _p(ent, _lib.c_double_p) if k1 > k0 else None
+    ck = None
+    if want_checkpoint:
+        nb = L.tessera_qa_checkpoint_bytes(n, chi)
+        ck = np.zeros(nb, np.uint8)
+        r.final_mps = ck.ctypes.data
+        r.final_mps_bytes = nb
+    rc = L.tessera_qa_anneal_ex(C.byref(P), C.byref(c), C.byref(r))
+    if rc != 0 and not (rc == _lib.ESTATUS and not raise_on_status):
+        raise _lib.EngineError(rc, _lib.last_error())
+    return AnnealResult(spins, r.energy, r.expected_energy, r.prob, r.max_trunc, r.norm2, ent[: k1 - k0],
+                        int(r.two_site_updates), int(r.status), int(r.max_sweeps), int(r.max_bond),
+                        float(r.device_ms), ck.tobytes() if ck is not None else None)
+
+
+def svd(a: np.ndarray):
+    """Thin SVD through the engine's Jacobi kernel (tessera_qa_svd): returns u, s, vh."""
+    L = _lib.load()
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    r, c = a.shape
+    k = min(r, c)
+    s = np.zeros(k)
+    u = np.zeros((r, k), np.complex128)
+    vh = np.zeros((k, c), np.complex128)
+    rc = L.tessera_qa_svd(a.view(np.float64).ctypes.data_as(_lib.c_double_p), r, c, s.ctypes.data_as(_lib.c_double_p),
+                          u.view(np.float64).ctypes.data_as(_lib.c_double_p),
+                          vh.view(np.float64).ctypes.data_as(_lib.c_double_p))
+    if rc != 0:
+        raise _lib.EngineError(rc, _lib.last_error())
+    return u, s, vh
+
+
+def checkpoint_to_sites(buf: bytes):
+    """Decode a checkpoint into (dims, [site tensors (Dl, 2, Dr) complex128])."""
+    raw = np.frombuffer(buf, dtype=np.uint8)
+    if raw[:8].tobytes() != b"TQMPSv1\x00":
+        raise ValueError("not a tessera_qa checkpoint")
+    n = int(np.frombuffer(raw[8:12].tobytes(), np.uint32)[0])
+    dims = np.frombuffer(raw[32:32 + 4 * (n + 1)].tobytes(), np.int32).copy()
+    off = 32 + (4 * (n + 1) + 7) // 8 * 8
+    sites = []
+    for i in range(n):
+        cnt = int(dims[i]) * 2 * int(dims[i + 1])
+        t = np.frombuffer(raw[off:off + 16 * cnt].tobytes(), np.complex128).reshape(dims[i], 2, dims[i + 1])
+        sites.append(t)
+        off += 16 * cnt
+    return dims, sites
+
+
+def sites_to_dense(sites) -> np.ndarray:
+    """Contract an MPS to its 2^n amplitudes; basis index bit i = physical index of site i."""
+    v = np.ones((1, 1), np.complex128)  # (configurations so far, bond)
+    for i, t in enumerate(sites):
+        # v[x, a] * t[a, s, b] -> w[x + s 2^i, b]
+        w = np.einsum("xa,asb->sxb", v, t)
+        v = w.reshape(-1, t.shape[2])
+    return v[:, 0]

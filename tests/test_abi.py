@@ -1,0 +1,111 @@
+"""The C ABI boundary, checked without a GPU: the library loads, exports every function that
+include/tessera_qa.h declares, and rejects invalid input before touching a device (the
+reference has no validation at all; cuda/src/ffi.cpp:10-37)."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from tessera_b200 import _lib, ffi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    txt = open(os.path.join(ROOT, "include", "tessera_qa.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(tessera_qa_\w+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.load()
+    names = header_functions()
+    assert "tessera_qa_anneal" in names and len(names) >= 10
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (\w+)", out))
+    for nme in names:
+        assert nme in exported, nme
+        getattr(L, nme)
+
+
+def test_legacy_symbol_signature_matches_rust_binding():
+    """rust/src/ffi.rs:21-34: (f64*, usize, usize*, usize*, f64*, usize, f64*, f64*, usize, usize, i8*, f64*) -> f64."""
+    L = _lib.load()
+    assert L.tessera_qa_anneal.restype is C.c_double
+    assert len(L.tessera_qa_anneal.argtypes) == 12
+
+
+def test_config_defaults_are_the_legacy_ones():
+    c, _ = ffi.config_struct()
+    assert c.dt == 0.1 and c.zz_substeps == 1 and c.chi == 32 and c.precision == 0
+
+
+def test_bad_schedule_rejected_like_rust():
+    m = ffi.Ising([1.0], [])
+    with pytest.raises(ffi.QaException) as e:
+        ffi.quantum_anneal(m, ffi.Schedule([1.0], [0.0]), 32)
+    assert e.value.err is ffi.QaError.BadSchedule
+
+
+@pytest.mark.parametrize("case", ["nan_h", "edge_oob", "chi0", "n0", "nan_sched", "bad_dt", "bad_block"])
+def test_invalid_input_returns_einval_without_a_gpu(case):
+    h = np.array([0.1, -0.2, 0.3])
+    ei, ej, ew = np.array([0, 1]), np.array([1, 2]), np.array([0.5, -0.5])
+    sa, sb = np.linspace(1, 0, 5), np.linspace(0, 1, 5)
+    kw = {}
+    if case == "nan_h":
+        h = np.array([np.nan, 0, 0])
+    elif case == "edge_oob":
+        ej = np.array([1, 3])
+    elif case == "chi0":
+        kw["chi"] = 0
+    elif case == "n0":
+        h = np.zeros(0)
+        ei, ej, ew = np.zeros(0), np.zeros(0), np.zeros(0)
+    elif case == "nan_sched":
+        sb = np.array([0, np.inf, 0.5, 0.7, 1.0])
+    elif case == "bad_dt":
+        kw["dt"] = -1.0
+    elif case == "bad_block":
+        kw["jacobi_block"] = 3
+    with pytest.raises(_lib.EngineError) as e:
+        ffi.anneal(h, ei, ej, ew, sa, sb, **kw)
+    assert e.value.code == _lib.EINVAL
+    assert len(_lib.last_error()) > 0
+
+
+def test_legacy_symbol_returns_nan_on_invalid_input():
+    L = _lib.load()
+    h = np.array([np.nan])
+    s = np.zeros(1, np.int8)
+    e = L.tessera_qa_anneal(h.ctypes.data_as(_lib.c_double_p), 1, None, None, None, 0, None, None, 0, 8,
+                            s.ctypes.data_as(_lib.c_int8_p), None)
+    assert np.isnan(e)
+    e = L.tessera_qa_anneal(h.ctypes.data_as(_lib.c_double_p), 1, None, None, None, 0, None, None, 0, 8, None, None)
+    assert np.isnan(e)
+
+
+def test_checkpoint_size_bound():
+    L = _lib.load()
+    assert L.tessera_qa_checkpoint_bytes(4, 2) >= 32 + 4 * 2 * 2 * 2 * 16
+
+
+def test_checkpoint_decoder_roundtrip():
+    # a hand-built 2-site checkpoint: dims [1, 2, 1]
+    n = 2
+    hdr = bytearray(32 + (4 * 3 + 7) // 8 * 8)
+    hdr[0:8] = b"TQMPSv1\x00"
+    hdr[8:12] = np.uint32(n).tobytes()
+    hdr[32:44] = np.array([1, 2, 1], np.int32).tobytes()
+    a = (np.arange(4) + 1j).astype(np.complex128).reshape(1, 2, 2)
+    b = (np.arange(4) - 2j).astype(np.complex128).reshape(2, 2, 1)
+    buf = bytes(hdr) + a.tobytes() + b.tobytes()
+    dims, sites = ffi.checkpoint_to_sites(buf)
+    assert list(dims) == [1, 2, 1]
+    assert np.allclose(sites[0], a) and np.allclose(sites[1], b)
+    psi = ffi.sites_to_dense(sites)
+    ref = np.array([(a[0, s0] @ b[:, s1, 0]) for s1 in range(2) for s0 in range(2)])
+    assert np.allclose(psi, ref)

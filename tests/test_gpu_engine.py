@@ -1,0 +1,181 @@
+"""Parity of the CUDA engine (through the C ABI) with the oracle and the reference.
+
+Tolerances (complex128 unless stated):
+* reference golden cases whose reference SVD is sound and which never truncate: energy,
+  <H>, prob rel 1e-9; entropy abs 1e-9.
+* reference golden cases whose reference SVD is sound and that truncate (chi below exact):
+  <H> rel 1e-4, entropy abs 1e-4, max_trunc rel 1e-2 -- the reference's own Gram-SVD
+  rounding (up to 1e-8 per update) accumulates to that level over the run.
+* every golden case against the oracle's accurate-SVD mode (same algorithm, keep rule,
+  gauge, gate order): spins equal, <H> rel 1e-6, entropy abs 1e-6.
+* exact chi against the exact state vector (engine's Trotter splitting): fidelity within 1e-8,
+  and the most probable bit pattern equal.
+* complex64 mode: <H> within 1e-4 relative of the complex128 engine, fidelity within 1e-6.
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import Instance, smooth_schedule
+from tessera_b200 import ffi, instances
+
+pytestmark = pytest.mark.gpu
+
+
+def schedule_of(spec):
+    kind, steps = spec
+    return smooth_schedule(steps) if kind == "smooth" else instances.linear(steps)
+
+
+def run_case(case, **kw):
+    d = case["instance"]
+    sa, sb = schedule_of(case["schedule"])
+    return ffi.anneal(d["h"], d["ei"], d["ej"], d["ew"], sa, sb, dt=case["dt"], chi=case["chi"],
+                      zz_substeps=case["zz_substeps"], **kw)
+
+
+def inst_of(d):
+    return Instance(np.array(d["h"]), np.array(d["ei"], dtype=np.int32), np.array(d["ej"], dtype=np.int32),
+                    np.array(d["ew"]))
+
+
+def fidelity(x, y):
+    return abs(np.vdot(x, y)) ** 2 / (np.vdot(x, x).real * np.vdot(y, y).real)
+
+
+def test_svd_kernel_matches_reference_spectra(golden):
+    for c in golden["svd"]:
+        A = (np.array(c["re"]) + 1j * np.array(c["im"])).reshape(c["rows"], c["cols"])
+        u, s, vh = ffi.svd(A)
+        assert np.allclose(s, c["s"], rtol=1e-10, atol=1e-12)
+        k = len(s)
+        assert np.linalg.norm(u.conj().T @ u - np.eye(k)) < 1e-12
+        assert np.linalg.norm(u @ np.diag(s) @ vh - A) < 1e-12 * np.linalg.norm(A) * max(A.shape)
+
+
+@pytest.mark.parametrize("shape", [(64, 64), (128, 96), (512, 512), (200, 300)])
+def test_svd_kernel_large_random(shape):
+    rng = np.random.Generator(np.random.PCG64(sum(shape)))
+    A = rng.normal(size=shape) + 1j * rng.normal(size=shape)
+    # give it a TEBD-like decaying spectrum
+    U, s, Vh = np.linalg.svd(A, full_matrices=False)
+    s = np.exp(-np.arange(len(s)) / 20.0)
+    A = (U * s) @ Vh
+    u, sg, vh = ffi.svd(A)
+    assert np.allclose(sg, s, rtol=1e-9, atol=1e-13)
+    assert np.linalg.norm(u @ np.diag(sg) @ vh - A) < 1e-11 * np.linalg.norm(A)
+
+
+def test_sound_reference_cases_match_the_reference(golden):
+    for case in golden["cases"]:
+        if not case["reference_svd_sound"]:
+            continue
+        r = run_case(case)
+        ref = case["out"]
+        truncating = "truncating" in case["tags"]
+        assert list(r.spins) == ref["spins"], case["name"]
+        assert r.energy == pytest.approx(ref["energy"], rel=1e-12, abs=1e-12), case["name"]
+        rt = 1e-4 if truncating else 1e-9
+        assert r.expected_energy == pytest.approx(ref["expected_energy"], rel=rt, abs=1e-10), case["name"]
+        assert np.max(np.abs(r.entropy - np.array(ref["entropy"]))) < (1e-4 if truncating else 1e-9), case["name"]
+        if truncating:
+            assert r.max_trunc == pytest.approx(ref["max_trunc"], rel=1e-2), case["name"]
+        else:
+            assert r.max_trunc < 1e-12 and ref["max_trunc"] < 1e-12
+        assert r.status == 0
+
+
+def test_every_golden_case_matches_the_accurate_oracle(oracle, golden):
+    for case in golden["cases"]:
+        sa, sb = schedule_of(case["schedule"])
+        o = oracle.mps_anneal(inst_of(case["instance"]), sa, sb, case["dt"], case["chi"], case["zz_substeps"],
+                              accurate_svd=True)
+        r = run_case(case)
+        assert list(r.spins) == list(o.spins), case["name"]
+        assert r.energy == pytest.approx(o.energy, abs=1e-10), case["name"]
+        assert r.expected_energy == pytest.approx(o.expected_energy, rel=1e-6, abs=1e-9), case["name"]
+        assert np.max(np.abs(r.entropy - o.entropy)) < 1e-6, case["name"]
+        if o.max_trunc > 1e-12:
+            assert r.max_trunc == pytest.approx(o.max_trunc, rel=1e-4), case["name"]
+        else:
+            assert r.max_trunc < 1e-12, case["name"]
+
+
+def _rand_small(n, seed):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    h = rng.uniform(-1, 1, n)
+    ei, ej, ew = [], [], []
+    for i in range(n):
+        for k in range(i + 1, n):
+            if rng.random() < 0.5:
+                ei.append(i); ej.append(k); ew.append(rng.uniform(-1, 1))
+    return Instance(h, np.array(ei, np.int32), np.array(ej, np.int32), np.array(ew))
+
+
+@pytest.mark.parametrize("n,seed", [(6, 1), (8, 2), (10, 3)])
+def test_exact_chi_state_matches_statevector(oracle, n, seed):
+    m = _rand_small(n, seed)
+    sa, sb = instances.linear(120)
+    chi = 1 << (n // 2)
+    r = ffi.anneal(m.h, m.ei, m.ej, m.ew, sa, sb, dt=0.1, chi=chi, want_checkpoint=True)
+    _, sites = ffi.checkpoint_to_sites(r.checkpoint)
+    psi = ffi.sites_to_dense(sites)
+    sv = oracle.sv_anneal(m, sa, sb, 0.1, mode=1, want_state=True)
+    assert 1 - fidelity(psi, sv.state) < 1e-8
+    assert r.expected_energy == pytest.approx(sv.expected_energy, abs=1e-8)
+    assert np.max(np.abs(r.entropy - sv.entropy)) < 1e-7
+    # most probable bit pattern (quantum.rs readout) equals the oracle's
+    best = int(np.argmax(np.abs(psi) ** 2))
+    spins = np.array([-1 if (best >> i) & 1 else 1 for i in range(n)])
+    assert list(spins) == list(sv.spins)
+    assert r.max_trunc < 1e-20
+    assert r.norm2 == pytest.approx(1.0, abs=1e-9)
+
+
+def test_legacy_symbol_through_rust_style_wrapper(oracle, golden):
+    lg = golden["legacy_abi"]
+    d = lg["instance"]
+    sa, sb = smooth_schedule(lg["schedule"][1])
+    model = ffi.Ising(d["h"], list(zip(d["ei"], d["ej"], d["ew"])))
+    res = ffi.quantum_anneal(model, ffi.Schedule(list(sa), list(sb)), lg["chi"])
+    o = oracle.mps_anneal(inst_of(d), sa, sb, 0.1, lg["chi"], accurate_svd=True)
+    assert list(res.spins) == list(o.spins)
+    assert res.energy == pytest.approx(o.energy, abs=1e-10)
+    assert np.max(np.abs(res.entropy - o.entropy)) < 1e-6
+
+
+def test_complex64_mode_error_is_bounded(oracle):
+    m = _rand_small(8, 7)
+    sa, sb = instances.linear(150)
+    r64 = ffi.anneal(m.h, m.ei, m.ej, m.ew, sa, sb, dt=0.1, chi=16, precision="c64", want_checkpoint=True)
+    sv = oracle.sv_anneal(m, sa, sb, 0.1, mode=1, want_state=True)
+    _, sites = ffi.checkpoint_to_sites(r64.checkpoint)
+    psi = ffi.sites_to_dense(sites)
+    assert 1 - fidelity(psi, sv.state) < 1e-6
+    assert r64.expected_energy == pytest.approx(sv.expected_energy, rel=1e-4)
+
+
+def test_checkpoint_resume_equals_straight_run():
+    p = instances.chain_range(n=12, dmax=2, seed=5, T=3.0, dt=0.05, chi=8, dist="normal", hzero=False)
+    full = ffi.anneal(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=8)
+    half = ffi.anneal(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=8, step_end=30, skip_observables=True,
+                      want_checkpoint=True)
+    rest = ffi.anneal(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=8, step_begin=30,
+                      initial_mps=half.checkpoint)
+    assert rest.expected_energy == pytest.approx(full.expected_energy, rel=1e-9)
+    assert list(rest.spins) == list(full.spins)
+    assert np.max(np.abs(np.concatenate([half.entropy, rest.entropy]) - full.entropy)) < 1e-9
+
+
+def test_chain16_chi32_against_statevector(oracle):
+    """Config-1 shape (n=16 chain, chi=32, linear schedule, dt=0.05) over the first 100 of its
+    400 steps, against the exact 2^16 state vector in the engine's splitting."""
+    p = instances.chain_nn(n=16, seed=1, T=20.0, dt=0.05, chi=32)
+    sa, sb = p.sa[:100], p.sb[:100]
+    r = ffi.anneal(p.h, p.ei, p.ej, p.ew, sa, sb, dt=p.dt, chi=32, want_checkpoint=True)
+    sv = oracle.sv_anneal(Instance(p.h, p.ei.astype(np.int32), p.ej.astype(np.int32), p.ew), sa, sb, p.dt,
+                          mode=1, want_state=True)
+    _, sites = ffi.checkpoint_to_sites(r.checkpoint)
+    psi = ffi.sites_to_dense(sites)
+    assert 1 - fidelity(psi, sv.state) < 1e-6
+    assert r.expected_energy == pytest.approx(sv.expected_energy, rel=1e-6)
+    assert np.max(np.abs(r.entropy - sv.entropy)) < 1e-6
