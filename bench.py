@@ -1,0 +1,337 @@
+#!/usr/bin/env python
+"""Benchmark: TEBD two-site updates/s at chi=256.
+
+Workload (one instance per GPU, "replicas only": the anneal of one instance does not
+shard): n=128 chain with couplings to neighbours at distances 1..4, J ~ U(-1,1), h = 0,
+linear schedule, T=50, dt=0.02 (2500 steps), chi=256, complex128, the reference's gate
+order (each ZZ edge through the swap network: 1998 two-site updates per Trotter step).
+A bench step is one second-order Trotter step at mid-anneal (s = 0.5), run on a
+device-resident MPS whose every bond is at its cap min(256, 2^i, 2^(n-i)): the MPS starts
+as a seeded random state so that every timed update is a saturated chi=256 update.
+
+  python bench.py [--gpus N --steps K --warmup W]            # libtessera_qa.so
+  python bench.py --impl reference [...]                     # the reference's CPU engine
+
+Printed: one JSON line on rank 0.  `value` = updates/s over all ranks with the MPS resident
+in HBM (CUDA events on the session stream, max over ranks); `e2e` = the same metric through
+the public C ABI tessera_qa_anneal_ex with host buffers (checkpoint in, checkpoint out);
+`roofline` = the Jacobi-SVD kernel's algorithmic bytes per launch over its average launch
+time; `cpu_baseline` = the reference engine timed on this host's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "TEBD two-site updates/s at chi=256"
+UNIT = "two-site updates/s"
+MID_STEP = 1250  # s = 1250/2499 ~ 0.5
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["tessera", "reference"], default="tessera")
+    ap.add_argument("--precision", choices=["c128", "c64"], default="c128")
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--dmax", type=int, default=4)
+    ap.add_argument("--chi", type=int, default=256)
+    ap.add_argument("--jacobi-block", type=int, default=0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="one untimed step only (for ncu); prints no bench line")
+    return ap.parse_args()
+
+
+def workload(args, rank=0):
+    from tessera_b200 import instances
+    p = instances.chain_range(n=args.n, dmax=args.dmax, seed=2 + rank, T=50.0, dt=0.02, chi=args.chi)
+    return p
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------------------------
+# clocks sampler (nvidia-smi during the timed region)
+# ------------------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev: int):
+        self.dev = dev
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-i", str(self.dev), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k] and "Not" not in r[5 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------------------------
+# reference CPU engine (oracle/_ref: the reference's own sources compiled here)
+# ------------------------------------------------------------------------------------
+def ref_svd_sample(m: int, threads: int, seed: int = 0):
+    """Wall time of `threads` concurrent reference tessera::svd calls on m x m complex matrices
+    with a TEBD-like decaying spectrum (one per thread; ctypes releases the GIL)."""
+    import numpy as np
+
+    from oracle.oracle import Reference
+    R = Reference()
+    rng = np.random.Generator(np.random.PCG64(seed))
+    mats = []
+    for _ in range(threads):
+        A = rng.normal(size=(m, m)) + 1j * rng.normal(size=(m, m))
+        U, _, Vh = np.linalg.svd(A)
+        mats.append((U * np.exp(-np.arange(m) / (m / 8))) @ Vh)
+    ths = [threading.Thread(target=R.svd, args=(a,)) for a in mats]
+    t0 = time.perf_counter()
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    return time.perf_counter() - t0
+
+
+class RefModel:
+    """Reference cost of one saturated chi=256 update: tessera::svd of a 512 x 512 theta is
+    >99% of MPS::apply_adjacent at that size (cuda/src/mps.cpp:41-100).  A step times m=256
+    (chi=128) SVDs on every host thread at once and extrapolates to m=512 with the cost
+    exponent between one m=128 SVD (timed once) and the m=256 batch."""
+
+    def __init__(self):
+        self.threads = max(1, min(len(os.sched_getaffinity(0)), 64))
+        self.t128 = ref_svd_sample(128, 1, seed=1)
+        self.p = 4.0
+
+    def step(self, seed=3):
+        import math
+        t = ref_svd_sample(256, self.threads, seed=seed)
+        self.p = math.log2(t / self.t128)
+        per_update_512 = t * 2.0 ** self.p
+        return t, self.threads / per_update_512
+
+    def describe(self, t):
+        return (f"{self.threads} concurrent reference tessera::svd calls on 256x256 complex128 theta "
+                f"(chi=128) took {t:.1f} s; extrapolated to the 512x512 theta of chi=256 with the "
+                f"measured cost exponent {self.p:.2f} (one 128x128 SVD -> the 256x256 batch)")
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle.oracle import Reference
+    if not Reference.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libtessera_ref.so was not built"}))
+        return
+    model = RefModel()
+    for w in range(args.warmup):
+        model.step(seed=10 + w)
+    vals, walls = [], []
+    for k in range(args.steps):
+        t, v = model.step(seed=100 + k)
+        vals.append(v)
+        walls.append(t)
+    value = statistics.mean(vals)
+    p = workload(args)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(walls),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config_dict(args, p),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": model.threads, "kind": "reference",
+                             "sample": model.describe(statistics.mean(walls))},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def config_dict(args, p):
+    return {"workload": f"chain n={args.n}, couplings at distances 1..{args.dmax}, J~U(-1,1), h=0, "
+                        f"linear schedule T=50 dt=0.02, chi={args.chi}, one Trotter step at s=0.5",
+            "n": args.n, "dmax": args.dmax, "chi": args.chi, "precision": args.precision,
+            "updates_per_step": p.updates_per_step(), "logical_zz_per_step": p.m,
+            "gate_order": "reference (edges in order, swap network, truncation after every swap)",
+            "l2": "inputs larger than L2 (MPS of 2*chi^2*16 B per site x n sites)",
+            "parallelism": "replicas" if args.gpus > 1 else "single GPU"}
+
+
+# ------------------------------------------------------------------------------------
+# tessera engine
+# ------------------------------------------------------------------------------------
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from tessera_b200 import ffi
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    p = workload(args, rank)
+    sess = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=args.chi, precision=args.precision,
+                       jacobi_block=args.jacobi_block, kernel_timing=True, device=local)
+    sess.randomize(1234 + rank)
+    upd_per_step = p.updates_per_step()
+    if args.profile_run:
+        sess.run(MID_STEP, 1)
+        r = sess.sync()
+        print(f"profile run: {r.two_site_updates} updates, status {r.status}, {r.device_ms:.1f} ms")
+        return
+    for w in range(args.warmup):
+        sess.run(MID_STEP - args.warmup + w, 1)
+    r0 = sess.sync()
+    stream = torch.cuda.ExternalStream(sess.stream)
+    clocks = Clocks(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sess.run(MID_STEP, args.steps)
+    e1.record(stream)
+    r1 = sess.sync()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    updates = r1.two_site_updates - r0.two_site_updates
+    assert updates == upd_per_step * args.steps, (updates, upd_per_step)
+    if r1.status:
+        raise RuntimeError(f"engine status bits {r1.status} during the timed steps")
+    value = updates * world / (ms_max / 1e3)
+    svd_n = r1.svd_launches - r0.svd_launches
+    svd_ms = r1.svd_ms - r0.svd_ms
+    svd_bytes = r1.svd_bytes - r0.svd_bytes
+    launches = r1.kernel_launches - r0.kernel_launches
+    sweeps = (r1.svd_sweeps - r0.svd_sweeps) / max(svd_n, 1)
+    peak, peak_kind = peaks()
+    achieved = (svd_bytes / svd_n) / (svd_ms / svd_n / 1e3) / 1e9 if svd_n else 0.0
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "k_svd_traffic.json")
+    if os.path.exists(tf):
+        try:
+            with open(tf) as f:
+                d = json.load(f)
+            if d.get("chi") == args.chi and d.get("precision") == args.precision:
+                traffic = d.get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    roofline = {"kernel": "k_svd (one-sided Jacobi SVD of theta, 512 x 512)", "bound": "hbm",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                "traffic": traffic, "avg_launch_ms": svd_ms / max(svd_n, 1),
+                "algorithmic_bytes_per_launch": svd_bytes / max(svd_n, 1), "avg_sweeps": sweeps,
+                "svd_share_of_step": svd_ms / ms if ms else None}
+
+    # ---- e2e through the public C ABI with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        ckpt = sess.save()  # current saturated state as a host checkpoint
+        pinned = torch.empty(len(ckpt), dtype=torch.uint8, pin_memory=True)
+        pinned.numpy()[:] = np.frombuffer(ckpt, np.uint8)
+        walls = []
+        h2d = len(ckpt) + p.h.nbytes + p.ew.nbytes + 2 * p.ei.nbytes + p.sa.nbytes + p.sb.nbytes
+        out = torch.empty(len(ckpt), dtype=torch.uint8, pin_memory=True)
+        d2h = len(ckpt) + 8 + 64  # final checkpoint (same dims), the step's entropy, result record
+        for k in range(1 + 1):  # one untimed call (allocation warm-up), one timed
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ffi.anneal(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=args.chi, precision=args.precision,
+                       step_begin=MID_STEP + k, step_end=MID_STEP + k + 1, skip_observables=True,
+                       initial_mps=pinned.numpy(), checkpoint_out=out.numpy(), device=local,
+                       jacobi_block=args.jacobi_block)
+            torch.cuda.synchronize()
+            walls.append(time.perf_counter() - t0)
+        e2e = {"value": upd_per_step * world / walls[-1], "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "api": "tessera_qa_anneal_ex (checkpoint in -> 1 Trotter step -> "
+                                                 "checkpoint out, host buffers)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle.oracle import Reference
+            if Reference.available():
+                model = RefModel()
+                tw, v = model.step()
+                cpu = {"value": v, "unit": UNIT, "cores": model.threads, "kind": "reference",
+                       "sample": model.describe(tw)}
+        except Exception as exc:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {exc}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "c128" else "f32",
+                "data": "synthetic: seeded Ising instance (PCG64 seed 2+rank) and seeded random MPS with every "
+                        "bond at its cap",
+                "config": config_dict(args, p), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches, "clocks": ck,
+                "logical_zz_gates_per_s": p.m * args.steps * world / (ms_max / 1e3),
+                "max_trunc_in_timed_steps": r1.max_trunc}
+        print(json.dumps(line))
+    sess.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -86,7 +86,8 @@ typedef struct tessera_qa_config {
     size_t step_end;        /* 0 = problem.steps */
     const void* initial_mps;/* NULL = |+>^n; else a checkpoint written by a previous call */
     int skip_observables;   /* 1 = skip the final <Z>, <ZZ>, readout and prob (checkpoint runs) */
-    int reserved[7];
+    int kernel_timing;      /* 1 = time every Jacobi-SVD launch with CUDA events (result.svd_ms) */
+    int reserved[6];
 } tessera_qa_config;
 
 typedef struct tessera_qa_result {
@@ -107,7 +108,14 @@ typedef struct tessera_qa_result {
     int max_bond;           /* largest bond dimension reached */
     int reserved_i;
     double device_ms;       /* GPU time of the Trotter steps (CUDA events) */
-    double reserved_d[4];
+    double min_cut_gap;     /* min over truncating updates of (s[keep-1] - s[keep]) / s[0]; 1 if none
+                               truncated.  Near 0 the kept subspace is not unique (degenerate cut). */
+    double svd_ms;          /* summed duration of the Jacobi-SVD launches (config.kernel_timing) */
+    double svd_bytes;       /* algorithmic bytes the Jacobi-SVD launches moved (see DESIGN) */
+    long long svd_launches; /* Jacobi-SVD launches */
+    long long svd_sweeps;   /* Jacobi sweeps summed over launches */
+    long long kernel_launches; /* all engine kernel launches */
+    double reserved_d[2];
 } tessera_qa_result;
 
 /* Fills `cfg` with the legacy defaults: dt 0.1, zz_substeps 1, complex128, chi 32. */

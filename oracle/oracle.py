@@ -114,7 +114,7 @@ class Oracle:
         n, steps = len(h), len(sa)
         spins = np.zeros(n, np.int8)
         ent = np.zeros(steps)
-        st = np.zeros(9)
+        st = np.zeros(10)
         state = np.zeros(2 << n) if want_state else None
         self.lib.orc_mps_anneal(_ptr(h, _dp), n, _ptr(ei, _ip), _ptr(ej, _ip), _ptr(ew, _dp), len(ew),
                                 _ptr(sa, _dp), _ptr(sb, _dp), steps, dt, chi, zz_substeps,
@@ -122,7 +122,8 @@ class Oracle:
                                 _ptr(state, _dp) if state is not None else None, 1 if accurate_svd else 0)
         return AnnealOut(spins, st[0], st[1], st[2], st[3], ent, int(st[4]), int(st[5]),
                          state.view(np.complex128) if state is not None else None,
-                         extra={"max_recon": st[6], "bad_updates": int(st[7]), "norm2": st[8]})
+                         extra={"max_recon": st[6], "bad_updates": int(st[7]), "norm2": st[8],
+                                "min_cut_gap": st[9]})
 
     def sv_anneal(self, inst: Instance, sa, sb, dt: float, mode: int = 0,
                   want_state: bool = False) -> AnnealOut:

@@ -305,6 +305,7 @@ struct Chain {
     double max_recon = 0.0;
     long long bad_updates = 0;
     int svd_mode = 0;  // 0: the reference's Gram-matrix SVD; 1: accurate one-sided Jacobi SVD
+    double min_gap = 1.0;  // min over truncating updates of (S[keep-1] - S[keep]) / S[0]
 
     explicit Chain(int n) : site(n) {  // |+>^n (cuda/src/mps.cpp:9-17)
         const double amp = 1.0 / std::sqrt(2.0);
@@ -378,6 +379,7 @@ struct Chain {
         while (keep > 1 && S[keep - 1] < 1e-14) --keep;
         double disc = 0.0;
         for (int t = keep; t < k; ++t) disc += S[t] * S[t];
+        if (keep < k && S[0] > 0) min_gap = std::min(min_gap, (S[keep - 1] - S[keep]) / S[0]);
         if (total > 0) max_trunc = std::max(max_trunc, disc / total);
         Tensor3 An(dl, keep), Cn(keep, dr);
         for (int a = 0; a < dl; ++a)
@@ -565,7 +567,7 @@ extern "C" {
 // Full MPS anneal (cuda/src/mps.cpp:295-381).  svd_mode 0 = the reference's Gram SVD
 // (bitwise the reference), 1 = accurate one-sided Jacobi SVD (same algorithm otherwise).  stats = {energy, expected_energy, prob,
 // max_trunc, two_site_updates, max_bond, max SVD reconstruction error, updates with a
-// reconstruction error above 1e-8, norm2}.  out_state: optional 2^n interleaved dense
+// reconstruction error above 1e-8, norm2, min relative gap at the truncation cut}.  out_state: optional 2^n interleaved dense
 // final state (unnormalised, as the MPS holds it).
 int orc_mps_anneal(const double* h, int n, const int* ei, const int* ej, const double* ew, int m,
                    const double* sa, const double* sb, int steps, double dt, int chi,
@@ -610,6 +612,7 @@ int orc_mps_anneal(const double* h, int n, const int* ei, const int* ej, const d
     stats[6] = psi.max_recon;
     stats[7] = (double)psi.bad_updates;
     stats[8] = psi.norm2();
+    stats[9] = psi.min_gap;
     if (out_state) psi.dense(reinterpret_cast<cplx*>(out_state));
     return 0;
 }

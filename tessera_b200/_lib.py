@@ -34,7 +34,8 @@ class Config(C.Structure):
     _fields_ = [("dt", C.c_double), ("zz_substeps", C.c_int), ("precision", C.c_int), ("chi", C.c_size_t),
                 ("jacobi_tol", C.c_double), ("jacobi_max_sweeps", C.c_int), ("jacobi_block", C.c_int),
                 ("device", C.c_int), ("step_begin", C.c_size_t), ("step_end", C.c_size_t),
-                ("initial_mps", C.c_void_p), ("skip_observables", C.c_int), ("reserved", C.c_int * 7)]
+                ("initial_mps", C.c_void_p), ("skip_observables", C.c_int), ("kernel_timing", C.c_int),
+                ("reserved", C.c_int * 6)]
 
 
 class Result(C.Structure):
@@ -43,7 +44,9 @@ class Result(C.Structure):
                 ("prob", C.c_double), ("max_trunc", C.c_double), ("norm2", C.c_double),
                 ("two_site_updates", C.c_longlong), ("status", C.c_int), ("max_sweeps", C.c_int),
                 ("max_bond", C.c_int), ("reserved_i", C.c_int), ("device_ms", C.c_double),
-                ("reserved_d", C.c_double * 4)]
+                ("min_cut_gap", C.c_double), ("svd_ms", C.c_double), ("svd_bytes", C.c_double),
+                ("svd_launches", C.c_longlong), ("svd_sweeps", C.c_longlong), ("kernel_launches", C.c_longlong),
+                ("reserved_d", C.c_double * 2)]
 
 
 _lib = None

@@ -124,6 +124,7 @@ struct Config {
     int block = 0;
     int device = -1;
     int min_ld = 0;  // workspace rows/cols at least this (standalone SVD)
+    int timing = 0;  // time each SVD launch with CUDA events
 };
 
 static Config validate_config(const tessera_qa_config* c) {
@@ -145,6 +146,7 @@ static Config validate_config(const tessera_qa_config* c) {
     C.max_sweeps = c->jacobi_max_sweeps ? c->jacobi_max_sweeps : 60;
     C.block = c->jacobi_block;
     C.device = c->device;
+    C.timing = c->kernel_timing;
     return C;
 }
 
@@ -191,6 +193,7 @@ public:
     }
     ~Engine() override {
         if (stream_) cudaStreamSynchronize(stream_);
+        for (cudaEvent_t e : pool_) cudaEventDestroy(e);
         if (ev0_) cudaEventDestroy(ev0_);
         if (ev1_) cudaEventDestroy(ev1_);
         if (base_) cudaFree(base_);
@@ -235,6 +238,7 @@ public:
             single_site(sch);
             entropy_step(M);
             launch_step_inc(step_, stream_);
+            launches_ += 5;  // two single-site, entropy chain, entropy, step counter
         }
         TQ_CK(cudaEventRecord(ev1_, stream_));
         ran_ = true;
@@ -250,13 +254,26 @@ public:
             TQ_CK(cudaEventElapsedTime(&ms, ev0_, ev1_));
             last_ms_ = ms;
         }
+        for (auto& pr : timed_) {
+            float ms = 0;
+            TQ_CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+            svd_ms_ += ms;
+        }
+        timed_.clear();
+        pool_next_ = 0;
         if (r) {
+            r->svd_ms = svd_ms_;
+            r->svd_bytes = st.svd_bytes;
+            r->svd_launches = svd_launches_;
+            r->svd_sweeps = st.svd_sweeps;
+            r->kernel_launches = launches_;
             r->max_trunc = st.max_trunc;
             r->two_site_updates = st.updates;
             r->status = st.status;
             r->max_sweeps = st.max_sweeps;
             r->max_bond = std::max(st.max_bond, 1);
             r->device_ms = last_ms_;
+            r->min_cut_gap = 1.0 - st.gap_deficit;
         }
     }
 
@@ -402,6 +419,7 @@ private:
     char* base_ = nullptr;
     V *sites_ = nullptr, *theta_ = nullptr, *W_ = nullptr, *envs_ = nullptr, *xs_ = nullptr, *vbuf_ = nullptr;
     int *dims_ = nullptr, *perm_ = nullptr, *counters_ = nullptr, *step_ = nullptr;
+    double* scal_ = nullptr;
     double *sig2_ = nullptr, *sig_ = nullptr, *h_ = nullptr, *w_ = nullptr, *sa_ = nullptr, *sb_ = nullptr;
     double *entropy_ = nullptr, *dotout_ = nullptr, *amp2_ = nullptr;
     int8_t* spins_d_ = nullptr;
@@ -415,16 +433,25 @@ private:
     std::vector<int> ub_;
     bool ran_ = false;
     double last_ms_ = 0.0;
+    long long launches_ = 0, svd_launches_ = 0;
+    double svd_ms_ = 0.0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timed_;
+    std::vector<cudaEvent_t> pool_;
+    size_t pool_next_ = 0;
 
     size_t site_stride() const { return (size_t)2 * cap_ * cap_; }
     MpsView<T> mps() const { return MpsView<T>{sites_, dims_, n_, cap_, (long long)site_stride()}; }
     ScheduleView schedule() const { return ScheduleView{h_, w_, sa_, sb_, step_, C_.dt, C_.dt / C_.ns}; }
-    SvdWork<T> work() const { return SvdWork<T>{theta_, W_, ld_, sig2_, sig_, perm_, counters_, bar_, stats_}; }
+    SvdWork<T> work() const { return SvdWork<T>{theta_, W_, ld_, sig2_, sig_, perm_, counters_, scal_, bar_, stats_}; }
 
     double tol_for(int R) const {
         if (C_.tol > 0) return C_.tol;
         const double eps = sizeof(T) == 8 ? 2.220446049250313e-16 : 1.1920928955078125e-07;
-        return sizeof(T) == 8 ? std::max(R, 16) * eps : 8.0 * std::sqrt((double)std::max(R, 16)) * eps;
+        // stop rotating a pair once |w_p^H w_q| <= tol |w_p||w_q|: 1e-13 in complex128 (a few
+        // hundred ulps above the rounding floor of the FP64 dot products), 8 sqrt(R) ulps of
+        // float in complex64 (whose dot products are accumulated in FP64)
+        return sizeof(T) == 8 ? std::max(1e-13, 4.0 * std::sqrt((double)R) * eps)
+                              : 8.0 * std::sqrt((double)std::max(R, 16)) * eps;
     }
 
     int pick_block(int R, int N) const {
@@ -483,6 +510,7 @@ private:
         add((void**)&sig_, sizeof(double) * ld_);
         add((void**)&perm_, sizeof(int) * ld_);
         add((void**)&counters_, sizeof(int) * C_.max_sweeps);
+        add((void**)&scal_, sizeof(double) * 2);
         add((void**)&bar_, sizeof(GridBar));
         add((void**)&stats_, sizeof(RunStats));
         add((void**)&h_, sizeof(double) * n_);
@@ -580,10 +608,31 @@ private:
         const int dl = ub_[i], dr = ub_[i + 2];
         const int keep_ub = std::min(C_.chi, std::min(2 * dl, 2 * dr));
         launch_theta<T>(M, sch, op, nullptr, work(), dl, dr, stream_);
+        cudaEvent_t a = nullptr, b = nullptr;
+        if (C_.timing) {
+            a = event();
+            b = event();
+            TQ_CK(cudaEventRecord(a, stream_));
+        }
         launch_svd<T>(M, i, C_.chi, tol_for(2 * dl), C_.max_sweeps, work(), 2 * dl, 2 * dr, pick_block(2 * dl, 2 * dr),
                       stream_);
+        if (C_.timing) {
+            TQ_CK(cudaEventRecord(b, stream_));
+            timed_.push_back({a, b});
+        }
         launch_absorb<T>(M, i, work(), 2 * dl, 2 * dr, keep_ub, stream_);
         ub_[i + 1] = keep_ub;
+        launches_ += 4;
+        ++svd_launches_;
+    }
+
+    cudaEvent_t event() {
+        if (pool_next_ < pool_.size()) return pool_[pool_next_++];
+        cudaEvent_t e;
+        TQ_CK(cudaEventCreate(&e));
+        pool_.push_back(e);
+        ++pool_next_;
+        return e;
     }
 
     void entropy_step(const MpsView<T>& M) {
@@ -808,6 +857,12 @@ int tessera_qa_session_sync(tessera_qa_session* s, tessera_qa_result* result) {
             result->max_sweeps = r.max_sweeps;
             result->max_bond = r.max_bond;
             result->device_ms = r.device_ms;
+            result->min_cut_gap = r.min_cut_gap;
+            result->svd_ms = r.svd_ms;
+            result->svd_bytes = r.svd_bytes;
+            result->svd_launches = r.svd_launches;
+            result->svd_sweeps = r.svd_sweeps;
+            result->kernel_launches = r.kernel_launches;
         }
         return 0;
     });

@@ -53,6 +53,9 @@ struct RunStats {
     int status;             // ST_* bits
     int max_bond;           // largest bond dimension seen
     int pad;
+    double gap_deficit;     // max over truncating updates of 1 - (s[keep-1] - s[keep]) / s[0]
+    double svd_bytes;       // algorithmic bytes moved by the Jacobi-SVD launches
+    long long svd_sweeps;   // sweeps summed over launches
 };
 
 // Per-update SVD workspace.
@@ -65,6 +68,7 @@ struct SvdWork {
     double* sig;        // sorted kept singular values [2cap]
     int* perm;          // sorted column order [2cap]
     int* counters;      // per-sweep rotation counts [max_sweeps]
+    double* scal;       // [2] scratch scalars (squared Frobenius norm of W), zeroed per launch
     GridBar* bar;
     RunStats* stats;
 };

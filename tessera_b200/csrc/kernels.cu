@@ -351,6 +351,29 @@ __global__ void __launch_bounds__(256) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdP
         return;
     }
     const int grp = tid / G;
+    // ||W||_F^2 first: columns whose squared norm is below the noise floor of the matrix
+    // (tiny) are never rotated, and the keep rule drops them.
+    {
+        const int warp = tid >> 5, lane = tid & 31;
+        double part = 0.0;
+        for (int j = blockIdx.x * 8 + warp; j < N; j += gridDim.x * 8) {
+            double sj = 0.0;
+            const V* w = W + (long long)j * ld;
+            for (int row = lane; row < R; row += 32) sj += (double)w[row].x * w[row].x + (double)w[row].y * w[row].y;
+            part += warp_sum(sj);
+        }
+        if (lane == 0) red[warp] = part;
+        __syncthreads();
+        if (tid == 0) {
+            double b = 0.0;
+            for (int w = 0; w < 8; ++w) b += red[w];
+            if (b != 0.0) atomicAdd(&wk.scal[0], b);
+        }
+    }
+    if (!grid_sync(wk.bar, status, nblk)) return;
+    const double fro2 = *(volatile double*)&wk.scal[0];
+    const double tiny = fmax(pp.tiny, sizeof(T) == 8 ? fmin(1e-28, 1e-30 * fro2) : 1e-13 * fro2);
+    const double keep_floor = sizeof(T) == 8 ? 1e-28 : fmax(1e-28, tiny);  // on sigma^2
     int sweep = 0;
     bool converged = false;
     for (; sweep < pp.max_sweeps; ++sweep) {
@@ -379,7 +402,7 @@ __global__ void __launch_bounds__(256) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdP
                         const int base = blk ? J * BW : I * BW;
                         const bool ok = (base + x < N) && (base + y < N);
                         rot += rotate_pair<T, G>(col + (blk * BW + x) * pp.rows_cap, col + (blk * BW + y) * pp.rows_cap,
-                                                 ok, R, pp.tol, pp.tiny, red, tid);
+                                                 ok, R, pp.tol, tiny, red, tid);
                         __syncthreads();
                     }
                 }
@@ -387,7 +410,7 @@ __global__ void __launch_bounds__(256) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdP
                     const int p = grp, q = (grp + t) % BW;
                     const bool ok = (I * BW + p < N) && (J * BW + q < N);
                     rot += rotate_pair<T, G>(col + p * pp.rows_cap, col + (BW + q) * pp.rows_cap, ok, R, pp.tol,
-                                             pp.tiny, red, tid);
+                                             tiny, red, tid);
                     __syncthreads();
                 }
                 if (rot && (tid % G) == 0) atomicAdd(&s_rot, rot);
@@ -455,7 +478,7 @@ __global__ void __launch_bounds__(256) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdP
     for (int e = tid; e < kk; e += 256) {
         const double v = key[e] > 0 ? key[e] : 0.0;
         tot += v;
-        if (e < keep0 && sqrt(v) >= 1e-14) big += 1.0;
+        if (e < keep0 && v >= keep_floor) big += 1.0;
     }
     tot = warp_sum(tot);
     big = warp_sum(big);
@@ -492,8 +515,17 @@ __global__ void __launch_bounds__(256) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdP
             if (ratio > st->max_trunc) st->max_trunc = ratio;
         }
         if (!isfinite(s_tot)) st->status |= ST_NONFINITE;
+        if (keep < kk && key[0] > 0) {
+            const double s0 = sqrt(key[0]), a = sqrt(fmax(key[keep - 1], 0.0)), b = sqrt(fmax(key[keep], 0.0));
+            const double deficit = 1.0 - (a - b) / s0;
+            if (deficit > st->gap_deficit) st->gap_deficit = deficit;
+        }
         if (!converged) st->status |= ST_JACOBI_NOT_CONVERGED;
         if (sweep > st->max_sweeps) st->max_sweeps = sweep;
+        st->svd_sweeps += sweep;
+        // staged reads + write-backs of every block pair in every round, plus the norm pre-pass
+        // and the final column norms
+        st->svd_bytes += ((double)sweep * (P - 1) * 2.0 + 2.0) * (double)R * N * sizeof(V);
         if (keep > st->max_bond) st->max_bond = keep;
         st->updates += 1;
         mps.dims[pp.bond + 1] = keep;
@@ -539,6 +571,7 @@ int launch_svd(const MpsView<T>& mps, int bond, int chi, double tol, int max_swe
     pp.rows_cap = (rows_ub + 7) & ~7;
     if (pp.rows_cap < 8) pp.rows_cap = 8;
     TQ_CHECK(cudaMemsetAsync(wk.counters, 0, sizeof(int) * max_sweeps, s));
+    TQ_CHECK(cudaMemsetAsync(wk.scal, 0, sizeof(double) * 2, s));
     switch (block_w) {
         case 1: return svd_launch_bw<T, 1>(mps, pp, wk, cols_ub, s);
         case 2: return svd_launch_bw<T, 2>(mps, pp, wk, cols_ub, s);

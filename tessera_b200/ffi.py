@@ -117,6 +117,7 @@ class AnnealResult:
     max_sweeps: int
     max_bond: int
     device_ms: float
+    min_cut_gap: float = 1.0
     checkpoint: bytes | None = None
     extra: dict = field(default_factory=dict)
 
@@ -151,15 +152,22 @@ def config_struct(dt=0.1, chi=32, precision="c128", zz_substeps=1, jacobi_tol=0.
     c.step_end = step_end
     keep = None
     if initial_mps is not None:
-        keep = np.frombuffer(initial_mps, dtype=np.uint8).copy()
+        if isinstance(initial_mps, np.ndarray) and initial_mps.flags["C_CONTIGUOUS"]:
+            keep = initial_mps  # used in place (e.g. a pinned host buffer)
+        else:
+            keep = np.frombuffer(initial_mps, dtype=np.uint8).copy()
         c.initial_mps = keep.ctypes.data
     c.skip_observables = 1 if skip_observables else 0
     return c, keep
 
 
 def anneal(h, ei, ej, ew, sa, sb, dt=0.1, chi=32, precision="c128", zz_substeps=1, want_checkpoint=False,
-           raise_on_status=True, **kw) -> AnnealResult:
-    """tessera_qa_anneal_ex: the MPS-TEBD anneal with every result field."""
+           raise_on_status=True, checkpoint_out: np.ndarray | None = None, **kw) -> AnnealResult:
+    """tessera_qa_anneal_ex: the MPS-TEBD anneal with every result field.
+
+    want_checkpoint returns the final MPS as checkpoint bytes; checkpoint_out (a contiguous uint8
+    array of at least tessera_qa_checkpoint_bytes(n, chi) bytes, e.g. pinned memory) receives it
+    in place instead."""
     L = _lib.load()
     P, keep = problem_struct(h, ei, ej, ew, sa, sb)
     c, keep2 = config_struct(dt=dt, chi=chi, precision=precision, zz_substeps=zz_substeps, **kw)
@@ -172,7 +180,10 @@ def anneal(h, ei, ej, ew, sa, sb, dt=0.1, chi=32, precision="c128", zz_substeps=
     r.spins = _p(spins, _lib.c_int8_p)
     r.entropy = _p(ent, _lib.c_double_p) if k1 > k0 else None
     ck = None
-    if want_checkpoint:
+    if checkpoint_out is not None:
+        r.final_mps = checkpoint_out.ctypes.data
+        r.final_mps_bytes = checkpoint_out.nbytes
+    elif want_checkpoint:
         nb = L.tessera_qa_checkpoint_bytes(n, chi)
         ck = np.zeros(nb, np.uint8)
         r.final_mps = ck.ctypes.data
@@ -182,7 +193,7 @@ def anneal(h, ei, ej, ew, sa, sb, dt=0.1, chi=32, precision="c128", zz_substeps=
         raise _lib.EngineError(rc, _lib.last_error())
     return AnnealResult(spins, r.energy, r.expected_energy, r.prob, r.max_trunc, r.norm2, ent[: k1 - k0],
                         int(r.two_site_updates), int(r.status), int(r.max_sweeps), int(r.max_bond),
-                        float(r.device_ms), ck.tobytes() if ck is not None else None)
+                        float(r.device_ms), float(r.min_cut_gap), ck.tobytes() if ck is not None else None)
 
 
 def svd(a: np.ndarray):
@@ -227,3 +238,67 @@ def sites_to_dense(sites) -> np.ndarray:
         w = np.einsum("xa,asb->sxb", v, t)
         v = w.reshape(-1, t.shape[2])
     return v[:, 0]
+
+
+class Session:
+    """A device-resident anneal (tessera_qa_session_*): the MPS stays in HBM between calls."""
+
+    def __init__(self, h, ei, ej, ew, sa, sb, dt=0.1, chi=32, precision="c128", zz_substeps=1,
+                 kernel_timing=False, **kw):
+        L = _lib.load()
+        self._L = L
+        self._P, self._keep = problem_struct(h, ei, ej, ew, sa, sb)
+        c, _ = config_struct(dt=dt, chi=chi, precision=precision, zz_substeps=zz_substeps, **kw)
+        c.kernel_timing = 1 if kernel_timing else 0
+        self.chi = chi
+        self.n = int(self._P.n)
+        self._h = L.tessera_qa_session_create(C.byref(self._P), C.byref(c))
+        if not self._h:
+            raise _lib.EngineError(_lib.ECUDA, _lib.last_error())
+
+    def _ck(self, rc):
+        if rc != 0:
+            raise _lib.EngineError(rc, _lib.last_error())
+
+    def randomize(self, seed: int):
+        self._ck(self._L.tessera_qa_session_randomize(self._h, seed))
+
+    def run(self, step_begin: int, nsteps: int):
+        self._ck(self._L.tessera_qa_session_run(self._h, step_begin, nsteps))
+
+    @property
+    def stream(self) -> int:
+        return int(self._L.tessera_qa_session_stream(self._h))
+
+    def sync(self) -> "_lib.Result":
+        r = _lib.Result()
+        self._ck(self._L.tessera_qa_session_sync(self._h, C.byref(r)))
+        return r
+
+    def observe(self, spins: np.ndarray | None = None) -> "_lib.Result":
+        r = _lib.Result()
+        if spins is not None:
+            r.spins = spins.ctypes.data_as(_lib.c_int8_p)
+        self._ck(self._L.tessera_qa_session_observe(self._h, C.byref(r)))
+        return r
+
+    def save(self) -> bytes:
+        nb = self._L.tessera_qa_checkpoint_bytes(self.n, self.chi)
+        buf = np.zeros(nb, np.uint8)
+        self._ck(self._L.tessera_qa_session_save(self._h, buf.ctypes.data, nb))
+        return buf.tobytes()
+
+    def load(self, buf: bytes):
+        a = np.frombuffer(buf, np.uint8).copy()
+        self._ck(self._L.tessera_qa_session_load(self._h, a.ctypes.data, a.size))
+
+    def close(self):
+        if self._h:
+            self._L.tessera_qa_session_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

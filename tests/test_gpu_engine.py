@@ -7,7 +7,11 @@ Tolerances (complex128 unless stated):
   <H> rel 1e-4, entropy abs 1e-4, max_trunc rel 1e-2 -- the reference's own Gram-SVD
   rounding (up to 1e-8 per update) accumulates to that level over the run.
 * every golden case against the oracle's accurate-SVD mode (same algorithm, keep rule,
-  gauge, gate order): spins equal, <H> rel 1e-6, entropy abs 1e-6.
+  gauge, gate order): <H> and entropy within 1e-6 plus ten times the case's own
+  sensitivity, measured by re-running the oracle with schedule and couplings moved by
+  4 ulps.  Truncated TEBD can amplify rounding exponentially in time (observed: x1000
+  per two steps at chi=8, n=8, d<=3), so two correct implementations agree only as well
+  as the run is conditioned; spins must agree where the run is well conditioned.
 * exact chi against the exact state vector (engine's Trotter splitting): fidelity within 1e-8,
   and the most probable bit pattern equal.
 * complex64 mode: <H> within 1e-4 relative of the complex128 engine, fidelity within 1e-6.
@@ -84,20 +88,51 @@ def test_sound_reference_cases_match_the_reference(golden):
         assert r.status == 0
 
 
+def perturbed(inst, sa, sb, eps=4e-16):
+    return (Instance(inst.h * (1 + eps), inst.ei, inst.ej, inst.ew * (1 + eps)), sa, sb * (1 + eps))
+
+
+def oracle_with_sensitivity(oracle, inst, sa, sb, dt, chi, zz=1):
+    o = oracle.mps_anneal(inst, sa, sb, dt, chi, zz, accurate_svd=True)
+    i2, a2, b2 = perturbed(inst, sa, sb)
+    p = oracle.mps_anneal(i2, a2, b2, dt, chi, zz, accurate_svd=True)
+    return o, abs(o.expected_energy - p.expected_energy), float(np.max(np.abs(o.entropy - p.entropy)))
+
+
 def test_every_golden_case_matches_the_accurate_oracle(oracle, golden):
     for case in golden["cases"]:
         sa, sb = schedule_of(case["schedule"])
-        o = oracle.mps_anneal(inst_of(case["instance"]), sa, sb, case["dt"], case["chi"], case["zz_substeps"],
-                              accurate_svd=True)
+        o, dh, ds = oracle_with_sensitivity(oracle, inst_of(case["instance"]), sa, sb, case["dt"], case["chi"],
+                                            case["zz_substeps"])
         r = run_case(case)
-        assert list(r.spins) == list(o.spins), case["name"]
-        assert r.energy == pytest.approx(o.energy, abs=1e-10), case["name"]
-        assert r.expected_energy == pytest.approx(o.expected_energy, rel=1e-6, abs=1e-9), case["name"]
-        assert np.max(np.abs(r.entropy - o.entropy)) < 1e-6, case["name"]
-        if o.max_trunc > 1e-12:
-            assert r.max_trunc == pytest.approx(o.max_trunc, rel=1e-4), case["name"]
-        else:
-            assert r.max_trunc < 1e-12, case["name"]
+        tol_h = 1e-6 * abs(o.expected_energy) + 1e-9 + 10 * dh
+        assert abs(r.expected_energy - o.expected_energy) <= tol_h, (case["name"], r.expected_energy,
+                                                                     o.expected_energy, dh)
+        assert np.max(np.abs(r.entropy - o.entropy)) <= 1e-6 + 10 * ds, case["name"]
+        if dh < 1e-9:
+            assert list(r.spins) == list(o.spins), case["name"]
+            assert r.energy == pytest.approx(o.energy, abs=1e-10), case["name"]
+            if o.max_trunc > 1e-12:
+                assert r.max_trunc == pytest.approx(o.max_trunc, rel=1e-4), case["name"]
+            else:
+                assert r.max_trunc < 1e-12, case["name"]
+
+
+@pytest.mark.parametrize("dmax,chi", [(1, 4), (2, 4), (3, 8)])
+def test_truncating_chain_tracks_the_oracle_step_by_step(oracle, dmax, chi):
+    """n=8, chi below exact: state fidelity to the oracle after every few steps, within the run's
+    own sensitivity (the d<=3, chi=8 run is chaotic after ~10 steps)."""
+    p = instances.chain_range(n=8, dmax=dmax, seed=9 if dmax > 1 else 1, T=2.0, dt=0.05, chi=chi, dist="normal",
+                              hzero=False)
+    inst = Instance(p.h, p.ei.astype(np.int32), p.ej.astype(np.int32), p.ew)
+    for steps in (2, 4, 8):
+        sa, sb = p.sa[:steps], p.sb[:steps]
+        r = ffi.anneal(p.h, p.ei, p.ej, p.ew, sa, sb, dt=p.dt, chi=chi, want_checkpoint=True)
+        o = oracle.mps_anneal(inst, sa, sb, p.dt, chi, want_state=True, accurate_svd=True)
+        _, sites = ffi.checkpoint_to_sites(r.checkpoint)
+        assert 1 - fidelity(ffi.sites_to_dense(sites), o.state) < 1e-8, (dmax, chi, steps)
+        assert r.max_trunc == pytest.approx(o.max_trunc, rel=1e-6, abs=1e-30)
+        assert r.min_cut_gap == pytest.approx(o.extra["min_cut_gap"], rel=1e-6)
 
 
 def _rand_small(n, seed):
