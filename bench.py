@@ -41,7 +41,7 @@ MID_STEP = 1250  # s = 1250/2499 ~ 0.5
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["tessera", "reference"], default="tessera")
     ap.add_argument("--precision", choices=["c128", "c64"], default="c128")

@@ -96,6 +96,7 @@ typedef struct tessera_qa_result {
     double* entropy;        /* step_end - step_begin values, qubit-0 entropy in bits */
     void* final_mps;        /* checkpoint buffer, tessera_qa_checkpoint_bytes() bytes */
     size_t final_mps_bytes;
+    double* z_expect;       /* n: <Z_i> of the final state (cuda/src/mps.cpp:182-186) */
     /* filled by the call */
     double energy;          /* Ising energy of `spins` */
     double expected_energy; /* <psi|H_problem|psi>/<psi|psi> from the MPS */

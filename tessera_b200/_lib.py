@@ -40,7 +40,7 @@ class Config(C.Structure):
 
 class Result(C.Structure):
     _fields_ = [("spins", c_int8_p), ("entropy", c_double_p), ("final_mps", C.c_void_p),
-                ("final_mps_bytes", C.c_size_t), ("energy", C.c_double), ("expected_energy", C.c_double),
+                ("final_mps_bytes", C.c_size_t), ("z_expect", c_double_p), ("energy", C.c_double), ("expected_energy", C.c_double),
                 ("prob", C.c_double), ("max_trunc", C.c_double), ("norm2", C.c_double),
                 ("two_site_updates", C.c_longlong), ("status", C.c_int), ("max_sweeps", C.c_int),
                 ("max_bond", C.c_int), ("reserved_i", C.c_int), ("device_ms", C.c_double),

@@ -69,14 +69,19 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
     return t;
 }
 
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
 __device__ __forceinline__ bool grid_sync(GridBar* bar, int* status, unsigned int nblocks,
                                           uint64_t budget_ns = 2000000000ull) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        volatile unsigned int* vgen = &bar->gen;
-        const unsigned int g = *vgen;
+        const unsigned int g = ld_acquire_u32(&bar->gen);
         __threadfence();
         const unsigned int arrived = atomicAdd(&bar->count, 1u);
         if (arrived == nblocks - 1) {
@@ -86,13 +91,12 @@ __device__ __forceinline__ bool grid_sync(GridBar* bar, int* status, unsigned in
         } else {
             const uint64_t t0 = globaltimer_ns();
             unsigned int spins = 0;
-            while (*vgen == g) {
-                if ((++spins & 63u) == 0 && globaltimer_ns() - t0 > budget_ns) {
+            while (ld_acquire_u32(&bar->gen) == g) {
+                if ((++spins & 255u) == 0 && globaltimer_ns() - t0 > budget_ns) {
                     atomicOr(status, ST_BARRIER_TIMEOUT);
                     ok = 0;
                     break;
                 }
-                __nanosleep(32);
             }
         }
         __threadfence();
@@ -101,6 +105,55 @@ __device__ __forceinline__ bool grid_sync(GridBar* bar, int* status, unsigned in
     }
     __syncthreads();
     return s_ok != 0;
+}
+
+// ---------------------------------------------------------------------------------
+// mbarrier + 1-D TMA bulk copies (cp.async.bulk, sm_90+; no tensor map, no multicast).
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// global -> shared bulk copy completing on `bar`; dst/src 16-byte aligned, bytes % 16 == 0.
+__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for phase `parity` of `bar`; returns false after budget_ns.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, uint64_t budget_ns) {
+    if (mbar_try_wait(bar, parity)) return true;
+    uint64_t t0 = 0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    for (;;) {
+        if (mbar_try_wait(bar, parity)) return true;
+        uint64_t t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (t - t0 > budget_ns) return false;
+    }
+}
+// Makes this thread's generic-proxy view of global memory consistent with async-proxy
+// (TMA) accesses issued after it.
+__device__ __forceinline__ void fence_proxy_async_global() {
+    asm volatile("fence.proxy.async.global;" ::: "memory");
 }
 
 // Warp-level sum with shuffles.

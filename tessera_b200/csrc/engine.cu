@@ -315,6 +315,7 @@ public:
             r->prob = nrm > 0 ? a2 / nrm : 0.0;
             r->norm2 = nrm;
             if (r->spins) std::memcpy(r->spins, spins.data(), n_);
+            if (r->z_expect) std::memcpy(r->z_expect, ez.data(), sizeof(double) * n_);
         }
     }
 

@@ -329,14 +329,22 @@ __device__ __forceinline__ void tournament(int P, int r, int pr, int& I, int& J)
     }
 }
 
+constexpr int SVD_THREADS = 512;
+
 template <typename T, int BW>
-__global__ void __launch_bounds__(256) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdParams pp) {
+__global__ void __launch_bounds__(SVD_THREADS, 1) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdParams pp) {
     using V = cplx_t<T>;
-    constexpr int G = 256 / BW;
+    constexpr int NT = SVD_THREADS;
+    constexpr int NW = NT / 32;
+    constexpr int G = NT / BW;
     extern __shared__ __align__(16) unsigned char smraw[];
     V* col = reinterpret_cast<V*>(smraw);  // [2*BW][rows_cap]
-    __shared__ double red[32];             // [8 warps][4]
+    __shared__ double red[4 * NW];         // [warps][4]
     __shared__ int s_rot;
+    __shared__ __align__(8) uint64_t s_mbar;
+    unsigned phase = 0;
+    if (threadIdx.x == 0) mbar_init(&s_mbar, 1);
+    __syncthreads();
     const int tid = threadIdx.x;
     const int R = pp.R > 0 ? pp.R : 2 * mps.dims[pp.bond];
     const int N = pp.N > 0 ? pp.N : 2 * mps.dims[pp.bond + 2];
@@ -356,7 +364,7 @@ __global__ void __launch_bounds__(256) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdP
     {
         const int warp = tid >> 5, lane = tid & 31;
         double part = 0.0;
-        for (int j = blockIdx.x * 8 + warp; j < N; j += gridDim.x * 8) {
+        for (int j = blockIdx.x * NW + warp; j < N; j += gridDim.x * NW) {
             double sj = 0.0;
             const V* w = W + (long long)j * ld;
             for (int row = lane; row < R; row += 32) sj += (double)w[row].x * w[row].x + (double)w[row].y * w[row].y;
@@ -366,14 +374,19 @@ __global__ void __launch_bounds__(256) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdP
         __syncthreads();
         if (tid == 0) {
             double b = 0.0;
-            for (int w = 0; w < 8; ++w) b += red[w];
+            for (int w = 0; w < NW; ++w) b += red[w];
             if (b != 0.0) atomicAdd(&wk.scal[0], b);
         }
     }
     if (!grid_sync(wk.bar, status, nblk)) return;
     const double fro2 = *(volatile double*)&wk.scal[0];
-    const double tiny = fmax(pp.tiny, sizeof(T) == 8 ? fmin(1e-28, 1e-30 * fro2) : 1e-13 * fro2);
-    const double keep_floor = sizeof(T) == 8 ? 1e-28 : fmax(1e-28, tiny);  // on sigma^2
+    // Noise floor: a column whose norm is below 8 sqrt(R) ulps of ||W||_F carries only rounding
+    // noise; it is frozen (never rotated) and dropped by the keep rule.  Rotating such columns
+    // against each other never converges and costs many sweeps on rank-deficient theta.
+    const double ulp = sizeof(T) == 8 ? 2.220446049250313e-16 : 1.1920928955078125e-07;
+    const double floor_rel = 8.0 * sqrt((double)R) * ulp;
+    const double tiny = fmax(pp.tiny, floor_rel * floor_rel * fro2);
+    const double keep_floor = fmax(1e-28, tiny);  // on sigma^2: the reference's 1e-14, or the noise floor
     int sweep = 0;
     bool converged = false;
     for (; sweep < pp.max_sweeps; ++sweep) {
@@ -381,14 +394,30 @@ __global__ void __launch_bounds__(256) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdP
             for (int pr = blockIdx.x; pr < P / 2; pr += gridDim.x) {
                 int I, J;
                 tournament(P, r, pr, I, J);
-                // stage columns: local c < BW -> block I, c >= BW -> block J
-                for (int e = tid; e < 2 * BW * R; e += 256) {
-                    const int c = e / R, row = e - c * R;
-                    const int gc = (c < BW) ? I * BW + c : J * BW + (c - BW);
-                    if (gc < N) col[c * pp.rows_cap + row] = W[(long long)gc * ld + row];
+                // stage columns with 1-D TMA bulk copies: local c < BW -> block I, c >= BW -> block J
+                if (tid == 0) {
+                    s_rot = 0;
+                    unsigned bytes = 0;
+                    for (int c = 0; c < 2 * BW; ++c) {
+                        const int gc = (c < BW) ? I * BW + c : J * BW + (c - BW);
+                        if (gc < N) bytes += (unsigned)(R * sizeof(V));
+                    }
+                    fence_proxy_async_global();
+                    mbar_expect_tx(&s_mbar, bytes);
+                    for (int c = 0; c < 2 * BW; ++c) {
+                        const int gc = (c < BW) ? I * BW + c : J * BW + (c - BW);
+                        if (gc < N)
+                            tma_load_1d(col + c * pp.rows_cap, W + (long long)gc * ld, (unsigned)(R * sizeof(V)),
+                                        &s_mbar);
+                    }
                 }
-                if (tid == 0) s_rot = 0;
-                __syncthreads();
+                if (!mbar_wait(&s_mbar, phase, 1000000000ull)) {
+                    atomicOr(status, ST_BARRIER_TIMEOUT);
+                    // keep waiting (bounded) for the copies in flight before leaving
+                    mbar_wait(&s_mbar, phase, 1000000000ull);
+                    return;
+                }
+                phase ^= 1u;
                 int rot = 0;
                 if constexpr (BW >= 2) if (r == 0) {
                     // intra-block pairs: circle method over BW columns, both blocks at once
@@ -415,10 +444,12 @@ __global__ void __launch_bounds__(256) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdP
                 }
                 if (rot && (tid % G) == 0) atomicAdd(&s_rot, rot);
                 __syncthreads();
-                for (int e = tid; e < 2 * BW * R; e += 256) {
-                    const int c = e / R, row = e - c * R;
+                for (int c = 0; c < 2 * BW; ++c) {
                     const int gc = (c < BW) ? I * BW + c : J * BW + (c - BW);
-                    if (gc < N) W[(long long)gc * ld + row] = col[c * pp.rows_cap + row];
+                    if (gc >= N) continue;
+                    V* dst = W + (long long)gc * ld;
+                    const V* src = col + c * pp.rows_cap;
+                    for (int row = tid; row < R; row += NT) dst[row] = src[row];
                 }
                 if (tid == 0 && s_rot) atomicAdd(&wk.counters[sweep], s_rot);
                 __syncthreads();
@@ -435,7 +466,7 @@ __global__ void __launch_bounds__(256) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdP
     // column norms -> sig2 (FP64)
     {
         const int warp = tid >> 5, lane = tid & 31;
-        for (int j = blockIdx.x * 8 + warp; j < N; j += gridDim.x * 8) {
+        for (int j = blockIdx.x * NW + warp; j < N; j += gridDim.x * NW) {
             double s = 0.0;
             const V* w = W + (long long)j * ld;
             for (int row = lane; row < R; row += 32) s += (double)w[row].x * w[row].x + (double)w[row].y * w[row].y;
@@ -450,14 +481,14 @@ __global__ void __launch_bounds__(256) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdP
     int* idx = reinterpret_cast<int*>(key + 4096);
     int P2 = 1;
     while (P2 < N) P2 <<= 1;
-    for (int e = tid; e < P2; e += 256) {
+    for (int e = tid; e < P2; e += NT) {
         key[e] = e < N ? wk.sig2[e] : -1.0;
         idx[e] = e;
     }
     __syncthreads();
     for (int k = 2; k <= P2; k <<= 1)
         for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int e = tid; e < P2; e += 256) {
+            for (int e = tid; e < P2; e += NT) {
                 const int o = e ^ j;
                 if (o > e) {
                     const bool desc = ((e & k) == 0);
@@ -475,7 +506,7 @@ __global__ void __launch_bounds__(256) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdP
     const int kk = R < N ? R : N;
     const int keep0 = pp.chi < kk ? pp.chi : kk;
     double tot = 0.0, big = 0.0;
-    for (int e = tid; e < kk; e += 256) {
+    for (int e = tid; e < kk; e += NT) {
         const double v = key[e] > 0 ? key[e] : 0.0;
         tot += v;
         if (e < keep0 && v >= keep_floor) big += 1.0;
@@ -488,7 +519,7 @@ __global__ void __launch_bounds__(256) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdP
     __shared__ double s_tot;
     if (tid == 0) {
         double t2 = 0.0, b2 = 0.0;
-        for (int w = 0; w < 8; ++w) { t2 += red[w * 4]; b2 += red[w * 4 + 1]; }
+        for (int w = 0; w < NW; ++w) { t2 += red[w * 4]; b2 += red[w * 4 + 1]; }
         int keep = pp.no_trunc ? kk : (int)b2;
         if (keep < 1) keep = 1;
         s_keep = keep;
@@ -497,18 +528,18 @@ __global__ void __launch_bounds__(256) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdP
     __syncthreads();
     const int keep = s_keep;
     double disc = 0.0;
-    for (int e = keep + tid; e < kk; e += 256) disc += key[e] > 0 ? key[e] : 0.0;
+    for (int e = keep + tid; e < kk; e += NT) disc += key[e] > 0 ? key[e] : 0.0;
     disc = warp_sum(disc);
     __syncthreads();
     if ((tid & 31) == 0) red[(tid >> 5) * 4 + 2] = disc;
-    for (int e = tid; e < keep; e += 256) {
+    for (int e = tid; e < keep; e += NT) {
         wk.perm[e] = idx[e];
         wk.sig[e] = sqrt(key[e] > 0 ? key[e] : 0.0);
     }
     __syncthreads();
     if (tid == 0 && !pp.no_trunc) {
         double d2 = 0.0;
-        for (int w = 0; w < 8; ++w) d2 += red[w * 4 + 2];
+        for (int w = 0; w < NW; ++w) d2 += red[w * 4 + 2];
         RunStats* st = wk.stats;
         if (s_tot > 0) {
             const double ratio = d2 / s_tot;
@@ -542,7 +573,7 @@ static int svd_launch_bw(const MpsView<T>& mps, const SvdParams& pp, SvdWork<T> 
     auto fn = k_svd<T, BW>;
     TQ_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    TQ_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, smem));
+    TQ_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, SVD_THREADS, smem));
     if (per_sm < 1) throw std::runtime_error("k_svd does not fit on an SM");
     const int nb = (cols_ub + BW - 1) / BW;
     const int pairs = (nb + (nb & 1)) / 2;
@@ -552,7 +583,7 @@ static int svd_launch_bw(const MpsView<T>& mps, const SvdParams& pp, SvdWork<T> 
     MpsView<T> m = mps;
     SvdParams p = pp;
     void* args[] = {&m, &wk, &p};
-    TQ_CHECK(cudaLaunchCooperativeKernel((const void*)fn, dim3(grid), dim3(256), args, smem, s));
+    TQ_CHECK(cudaLaunchCooperativeKernel((const void*)fn, dim3(grid), dim3(SVD_THREADS), args, smem, s));
     return grid;
 }
 

@@ -119,6 +119,7 @@ class AnnealResult:
     device_ms: float
     min_cut_gap: float = 1.0
     checkpoint: bytes | None = None
+    z_expect: np.ndarray | None = None
     extra: dict = field(default_factory=dict)
 
 
@@ -178,6 +179,8 @@ def anneal(h, ei, ej, ew, sa, sb, dt=0.1, chi=32, precision="c128", zz_substeps=
     ent = np.zeros(max(k1 - k0, 1), np.float64)
     r = _lib.Result()
     r.spins = _p(spins, _lib.c_int8_p)
+    zexp = np.zeros(n, np.float64)
+    r.z_expect = _p(zexp, _lib.c_double_p)
     r.entropy = _p(ent, _lib.c_double_p) if k1 > k0 else None
     ck = None
     if checkpoint_out is not None:
@@ -193,7 +196,8 @@ def anneal(h, ei, ej, ew, sa, sb, dt=0.1, chi=32, precision="c128", zz_substeps=
         raise _lib.EngineError(rc, _lib.last_error())
     return AnnealResult(spins, r.energy, r.expected_energy, r.prob, r.max_trunc, r.norm2, ent[: k1 - k0],
                         int(r.two_site_updates), int(r.status), int(r.max_sweeps), int(r.max_bond),
-                        float(r.device_ms), float(r.min_cut_gap), ck.tobytes() if ck is not None else None)
+                        float(r.device_ms), float(r.min_cut_gap), ck.tobytes() if ck is not None else None,
+                        zexp)
 
 
 def svd(a: np.ndarray):
