@@ -137,6 +137,20 @@ TESSERA_QA_API size_t tessera_qa_checkpoint_bytes(size_t n, size_t chi);
  * reference's tessera::svd (cuda/src/linalg.cpp:107-172). */
 TESSERA_QA_API int tessera_qa_svd(const double* a, size_t rows, size_t cols, double* s, double* u, double* vh);
 
+/* Allocation-free SVD, for callers that cannot call cudaMalloc (their device memory belongs to
+ * a host application's or framework's allocator, or allocation is forbidden after start-up).
+ * No counterpart in the reference.  Same one-sided Jacobi kernel as tessera_qa_svd, but
+ * d_a (rows x cols complex128, row-major interleaved re/im), d_s (min(rows,cols) singular
+ * values, descending) and d_u (rows x k left singular vectors, row-major; may be NULL) are
+ * DEVICE pointers on the current device, and all scratch is a fixed file-scope device array:
+ * rows and cols must be 1..256 (larger sizes return TESSERA_QA_EINVAL), and no device memory
+ * is allocated or freed.  Work is ordered on `stream` (a cudaStream_t; NULL = legacy default
+ * stream) and the call waits for it before returning.  The first call on each device sets
+ * the array up (device-address lookup, kernel load); make it before any stream capture.
+ * All calls share the one array: calls that overlap on the GPU race and must be serialised. */
+TESSERA_QA_API int tessera_qa_svd_noalloc(const double* d_a, size_t rows, size_t cols, double* d_s, double* d_u,
+                                          void* stream);
+
 /* Copies the calling thread's last error message into buf; returns its full length. */
 TESSERA_QA_API int tessera_qa_last_error(char* buf, size_t len);
 

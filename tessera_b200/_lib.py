@@ -76,6 +76,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.tessera_qa_checkpoint_bytes.restype = C.c_size_t
         L.tessera_qa_svd.argtypes = [c_double_p, C.c_size_t, C.c_size_t, c_double_p, c_double_p, c_double_p]
         L.tessera_qa_svd.restype = C.c_int
+        L.tessera_qa_svd_noalloc.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_void_p,
+                                             C.c_void_p]
+        L.tessera_qa_svd_noalloc.restype = C.c_int
         L.tessera_qa_last_error.argtypes = [C.c_char_p, C.c_size_t]
         L.tessera_qa_last_error.restype = C.c_int
         L.tessera_qa_session_create.argtypes = [C.POINTER(Problem), C.POINTER(Config)]

@@ -42,6 +42,7 @@ struct ArgError : std::runtime_error {
 static thread_local std::string t_err;
 
 static void set_err(const std::string& s) { t_err = s; }
+void set_last_error(const std::string& msg) { t_err = msg; }
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
