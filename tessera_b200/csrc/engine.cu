@@ -461,10 +461,9 @@ private:
         if (!b) {
             // default schedule: wide blocks for small matrices (few grid barriers), narrower
             // ones for large matrices (enough block pairs to fill the SMs)
-            if (N <= 32) b = 16;
-            else if (N <= 128) b = 8;
-            else if (N <= 512) b = 4;
-            else b = 4;
+            if (N <= 64) b = 16;
+            else if (N <= 256) b = 8;
+            else b = 8;
         }
         const int rows_cap = (R + 7) & ~7;
         while (b > 1 && (size_t)2 * b * rows_cap * sizeof(V) > 200 * 1024) b >>= 1;

@@ -331,10 +331,21 @@ __device__ __forceinline__ void tournament(int P, int r, int pr, int& I, int& J)
 
 constexpr int SVD_THREADS = 512;
 
-template <typename T, int BW>
-__global__ void __launch_bounds__(SVD_THREADS, 1) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdParams pp) {
+// RPL = 0: shared-memory rotations, SVD_THREADS threads, G = SVD_THREADS/BW threads per pair.
+// RPL > 0: register-resident cross rounds, one warp per pair (NT = 32 BW threads): warp w keeps
+//          column w of block I in registers (RPL complex rows per lane, R <= 32 RPL) for all BW
+//          inner rounds and streams the J columns through shared memory, so a cross rotation
+//          reads and writes one column of shared memory instead of two, and reduces with warp
+//          shuffles only.
+template <int BW, int RPL>
+struct SvdShape {
+    static constexpr int NT = RPL > 0 ? 32 * BW : SVD_THREADS;
+};
+
+template <typename T, int BW, int RPL>
+__global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdParams pp) {
     using V = cplx_t<T>;
-    constexpr int NT = SVD_THREADS;
+    constexpr int NT = SvdShape<BW, RPL>::NT;
     constexpr int NW = NT / 32;
     constexpr int G = NT / BW;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -435,11 +446,80 @@ __global__ void __launch_bounds__(SVD_THREADS, 1) k_svd(MpsView<T> mps, SvdWork<
                         __syncthreads();
                     }
                 }
-                for (int t = 0; t < BW; ++t) {
-                    const int p = grp, q = (grp + t) % BW;
-                    const bool ok = (I * BW + p < N) && (J * BW + q < N);
-                    rot += rotate_pair<T, G>(col + p * pp.rows_cap, col + (BW + q) * pp.rows_cap, ok, R, pp.tol,
-                                             tiny, red, tid);
+                if constexpr (RPL == 0) {
+                    for (int t = 0; t < BW; ++t) {
+                        const int p = grp, q = (grp + t) % BW;
+                        const bool ok = (I * BW + p < N) && (J * BW + q < N);
+                        rot += rotate_pair<T, G>(col + p * pp.rows_cap, col + (BW + q) * pp.rows_cap, ok, R, pp.tol,
+                                                 tiny, red, tid);
+                        __syncthreads();
+                    }
+                } else {
+                    static_assert(G == 32, "register path: one warp per pair");
+                    const int lane = tid & 31;
+                    const bool vi = I * BW + grp < N;
+                    V* ci = col + grp * pp.rows_cap;
+                    V xi[RPL];
+#pragma unroll
+                    for (int k = 0; k < RPL; ++k) {
+                        const int row = lane + 32 * k;
+                        xi[k] = (row < R) ? ci[row] : czero<V>();
+                    }
+                    for (int t = 0; t < BW; ++t) {
+                        const int q = (grp + t) % BW;
+                        const bool ok = vi && (J * BW + q < N);
+                        V* cq = col + (BW + q) * pp.rows_cap;
+                        V yj[RPL];
+#pragma unroll
+                        for (int k = 0; k < RPL; ++k) {
+                            const int row = lane + 32 * k;
+                            yj[k] = (row < R) ? cq[row] : czero<V>();
+                        }
+                        double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+#pragma unroll
+                        for (int k = 0; k < RPL; ++k) {
+                            const V x = xi[k], y = yj[k];
+                            v0 += (double)x.x * x.x + (double)x.y * x.y;
+                            v1 += (double)y.x * y.x + (double)y.y * y.y;
+                            v2 += (double)x.x * y.x + (double)x.y * y.y;
+                            v3 += (double)x.x * y.y - (double)x.y * y.x;
+                        }
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) {
+                            v0 += __shfl_xor_sync(0xffffffffu, v0, o);
+                            v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+                            v2 += __shfl_xor_sync(0xffffffffu, v2, o);
+                            v3 += __shfl_xor_sync(0xffffffffu, v3, o);
+                        }
+                        const double g = sqrt(v2 * v2 + v3 * v3);
+                        if (ok && v0 > tiny && v1 > tiny && g > pp.tol * sqrt(v0 * v1)) {
+                            const double zeta = (v1 - v0) / (2.0 * g);
+                            const double tt = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                            const double cs = 1.0 / sqrt(1.0 + tt * tt);
+                            const T c = (T)cs, sn = (T)(cs * tt);
+                            const T er = (T)(v2 / g), ei = (T)(v3 / g);
+#pragma unroll
+                            for (int k = 0; k < RPL; ++k) {
+                                const V x = xi[k], y = yj[k];
+                                const T ey_re = er * y.x + ei * y.y, ey_im = er * y.y - ei * y.x;
+                                const T ex_re = er * x.x - ei * x.y, ex_im = er * x.y + ei * x.x;
+                                xi[k] = mk<V>(c * x.x - sn * ey_re, c * x.y - sn * ey_im);
+                                yj[k] = mk<V>(sn * ex_re + c * y.x, sn * ex_im + c * y.y);
+                            }
+#pragma unroll
+                            for (int k = 0; k < RPL; ++k) {
+                                const int row = lane + 32 * k;
+                                if (row < R) cq[row] = yj[k];
+                            }
+                            if (lane == 0) ++rot;
+                        }
+                        __syncthreads();
+                    }
+#pragma unroll
+                    for (int k = 0; k < RPL; ++k) {
+                        const int row = lane + 32 * k;
+                        if (row < R) ci[row] = xi[k];
+                    }
                     __syncthreads();
                 }
                 if (rot && (tid % G) == 0) atomicAdd(&s_rot, rot);
@@ -563,17 +643,18 @@ __global__ void __launch_bounds__(SVD_THREADS, 1) k_svd(MpsView<T> mps, SvdWork<
     }
 }
 
-template <typename T, int BW>
+template <typename T, int BW, int RPL>
 static int svd_launch_bw(const MpsView<T>& mps, const SvdParams& pp, SvdWork<T> wk, int cols_ub,
                          cudaStream_t s) {
     using V = cplx_t<T>;
+    constexpr int NT = SvdShape<BW, RPL>::NT;
     size_t smem = sizeof(V) * 2 * BW * (size_t)pp.rows_cap;
     const size_t sort_smem = 4096 * (sizeof(double) + sizeof(int));
     if (smem < sort_smem) smem = sort_smem;
-    auto fn = k_svd<T, BW>;
+    auto fn = k_svd<T, BW, RPL>;
     TQ_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    TQ_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, SVD_THREADS, smem));
+    TQ_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, NT, smem));
     if (per_sm < 1) throw std::runtime_error("k_svd does not fit on an SM");
     const int nb = (cols_ub + BW - 1) / BW;
     const int pairs = (nb + (nb & 1)) / 2;
@@ -583,7 +664,7 @@ static int svd_launch_bw(const MpsView<T>& mps, const SvdParams& pp, SvdWork<T> 
     MpsView<T> m = mps;
     SvdParams p = pp;
     void* args[] = {&m, &wk, &p};
-    TQ_CHECK(cudaLaunchCooperativeKernel((const void*)fn, dim3(grid), dim3(SVD_THREADS), args, smem, s));
+    TQ_CHECK(cudaLaunchCooperativeKernel((const void*)fn, dim3(grid), dim3(NT), args, smem, s));
     return grid;
 }
 
@@ -603,13 +684,24 @@ int launch_svd(const MpsView<T>& mps, int bond, int chi, double tol, int max_swe
     if (pp.rows_cap < 8) pp.rows_cap = 8;
     TQ_CHECK(cudaMemsetAsync(wk.counters, 0, sizeof(int) * max_sweeps, s));
     TQ_CHECK(cudaMemsetAsync(wk.scal, 0, sizeof(double) * 2, s));
+    // register-resident path for rows <= 512: rows per lane = next power of two >= rows/32
+    int rpl = 1;
+    while (32 * rpl < pp.rows_cap) rpl <<= 1;
+    if (rpl <= 16) {
+        int bw = block_w < 4 ? 4 : block_w;
+        if (rpl == 16 && bw > 8) bw = 8;  // registers: 2 columns x 16 rows per lane
+#define TQ_RR(B, RP) \
+    if (bw == B && rpl == RP) return svd_launch_bw<T, B, RP>(mps, pp, wk, cols_ub, s);
+        TQ_RR(4, 1) TQ_RR(4, 2) TQ_RR(4, 4) TQ_RR(4, 8) TQ_RR(4, 16)
+        TQ_RR(8, 1) TQ_RR(8, 2) TQ_RR(8, 4) TQ_RR(8, 8) TQ_RR(8, 16)
+        TQ_RR(16, 1) TQ_RR(16, 2) TQ_RR(16, 4) TQ_RR(16, 8)
+#undef TQ_RR
+        throw std::runtime_error("unsupported Jacobi block width");
+    }
     switch (block_w) {
-        case 1: return svd_launch_bw<T, 1>(mps, pp, wk, cols_ub, s);
-        case 2: return svd_launch_bw<T, 2>(mps, pp, wk, cols_ub, s);
-        case 4: return svd_launch_bw<T, 4>(mps, pp, wk, cols_ub, s);
-        case 8: return svd_launch_bw<T, 8>(mps, pp, wk, cols_ub, s);
-        case 16: return svd_launch_bw<T, 16>(mps, pp, wk, cols_ub, s);
-        default: throw std::runtime_error("unsupported Jacobi block width");
+        case 1:
+        case 2: return svd_launch_bw<T, 2, 0>(mps, pp, wk, cols_ub, s);
+        default: return svd_launch_bw<T, 4, 0>(mps, pp, wk, cols_ub, s);
     }
 }
 

@@ -112,7 +112,7 @@ extern "C" int tessera_qa_svd_noalloc(const double* d_a, size_t rows, size_t col
         SvdWork<double> wk{nullptr, sc->W, kNoAllocMaxDim, sc->sig2, sc->sig, sc->perm,
                            sc->counters, sc->scal, &sc->bar, &sc->stats};
         MpsView<double> none{nullptr, nullptr, 0, 1, 0};
-        const int bw = N <= 32 ? 16 : (N <= 128 ? 8 : 4);
+        const int bw = N <= 64 ? 16 : 8;
         const double tol = 1e-13;
         launch_svd<double>(none, 0, k, tol, kNoAllocSweeps, wk, R, N, bw, s, R, N);
         k_noalloc_store<<<(R * k + 255) / 256, 256, 0, s>>>(sc->W, sc->perm, sc->sig, R, k, d_s,
