@@ -128,6 +128,15 @@ TESSERA_QA_API void tessera_qa_config_init(tessera_qa_config* cfg);
 TESSERA_QA_API int tessera_qa_anneal_ex(const tessera_qa_problem* problem, const tessera_qa_config* config,
                          tessera_qa_result* result);
 
+/* Batched anneal of `count` independent instances (the north_star batching layer): each
+ * instance runs exactly its own tessera_qa_anneal_ex (same gate order, keep rule, results),
+ * but gate slot q of every instance goes into one launch of each batched kernel, with one
+ * CTA per Jacobi SVD, so many updates run concurrently.  Instances may differ in n, edges,
+ * chi and dt; they must share precision and number of schedule steps, and start from |+>^n.
+ * No counterpart in the reference, which anneals one instance per call. */
+TESSERA_QA_API int tessera_qa_anneal_batch(const tessera_qa_problem* problems, const tessera_qa_config* configs,
+                                           tessera_qa_result* results, size_t count);
+
 /* Bytes of a checkpoint for n sites at bond cap chi (upper bound; any dims fit). */
 TESSERA_QA_API size_t tessera_qa_checkpoint_bytes(size_t n, size_t chi);
 

@@ -72,6 +72,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.tessera_qa_config_init.restype = None
         L.tessera_qa_anneal_ex.argtypes = [C.POINTER(Problem), C.POINTER(Config), C.POINTER(Result)]
         L.tessera_qa_anneal_ex.restype = C.c_int
+        L.tessera_qa_anneal_batch.argtypes = [C.POINTER(Problem), C.POINTER(Config), C.POINTER(Result), C.c_size_t]
+        L.tessera_qa_anneal_batch.restype = C.c_int
         L.tessera_qa_checkpoint_bytes.argtypes = [C.c_size_t, C.c_size_t]
         L.tessera_qa_checkpoint_bytes.restype = C.c_size_t
         L.tessera_qa_svd.argtypes = [c_double_p, C.c_size_t, C.c_size_t, c_double_p, c_double_p, c_double_p]

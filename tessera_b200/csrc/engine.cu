@@ -411,6 +411,40 @@ public:
     }
     int status_ = 0;
     int cap() const { return cap_; }
+    int n() const { return n_; }
+    const std::vector<GateOp>& ops() const { return ops_; }
+    // Device views of this instance for the batched kernels; `step` is the batch's shared
+    // step counter, `rows_cap` the batch-wide shared-memory column length.
+    InstTask<T> inst_task(int* step, int rows_cap) const {
+        InstTask<T> t;
+        t.mps = mps();
+        t.sch = schedule();
+        t.sch.step = step;
+        t.wk = work();
+        t.pp.bond = 0;
+        t.pp.R = 0;
+        t.pp.N = 0;
+        t.pp.no_trunc = 0;
+        t.pp.chi = C_.chi;
+        t.pp.tol = tol_for(2 * cap_);
+        t.pp.tiny = sizeof(T) == 8 ? 1e-200 : 1e-60;
+        t.pp.max_sweeps = C_.max_sweeps;
+        t.pp.rows_cap = rows_cap;
+        t.ent_steps = entc_;
+        t.n_ent = n_ent_;
+        t.pad = 0;
+        t.envs = envs_;
+        t.X = xs_;
+        t.r1_off = r1_off_;
+        t.entropy = entropy_;
+        return t;
+    }
+    void reset_counters() { TQ_CK(cudaMemsetAsync(counters_, 0, sizeof(int) * C_.max_sweeps, stream_)); }
+    void mark_ran(double ms) { ran_ = false; last_ms_ = ms; }
+    int max_sweeps_cfg() const { return C_.max_sweeps; }
+    int* counters_ptr() const { return counters_; }
+    double* scal_ptr() const { return scal_; }
+    cudaStream_t own_stream() const { return stream_; }
 
 private:
     ProblemHost P_;
@@ -654,6 +688,125 @@ static std::unique_ptr<EngineBase> make_engine(const ProblemHost& P, const Confi
     return std::unique_ptr<EngineBase>(new Engine<double>(P, C));
 }
 
+// Many independent instances annealed in lock step: gate slot q of every instance that has
+// one goes into one launch of each batched kernel (theta, one-CTA-per-task Jacobi SVD,
+// absorption), so each instance keeps the reference's gate order while the GPU is filled
+// with independent SVDs.
+template <typename T>
+class BatchEngine {
+public:
+    BatchEngine(const std::vector<ProblemHost>& P, const std::vector<Config>& C) {
+        const int B = (int)P.size();
+        int steps = 0;
+        for (int b = 0; b < B; ++b) {
+            eng_.emplace_back(new Engine<T>(P[b], C[b]));
+            steps = std::max(steps, P[b].steps);
+            cap_max_ = std::max(cap_max_, eng_.back()->cap());
+            n_max_ = std::max(n_max_, eng_.back()->n());
+            q_max_ = std::max(q_max_, (int)eng_.back()->ops().size());
+        }
+        steps_ = steps;
+        block_ = C[0].block ? C[0].block : (2 * cap_max_ <= 64 ? 16 : 8);
+        rows_cap_ = std::max(8, (2 * cap_max_ + 7) & ~7);
+        TQ_CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+        TQ_CK(cudaEventCreate(&e0_));
+        TQ_CK(cudaEventCreate(&e1_));
+        // device: shared step counter, instance views, per-slot update lists
+        size_t nref_tot = 0;
+        refs_off_.assign(q_max_ + 1, 0);
+        std::vector<UpdRef> refs;
+        for (int q = 0; q < q_max_; ++q) {
+            refs_off_[q] = refs.size();
+            for (int b = 0; b < B; ++b)
+                if (q < (int)eng_[b]->ops().size()) refs.push_back(UpdRef{b, eng_[b]->ops()[q]});
+        }
+        refs_off_[q_max_] = refs.size();
+        nref_tot = refs.size();
+        const size_t bytes = 256 + sizeof(InstTask<T>) * B + sizeof(UpdRef) * std::max<size_t>(nref_tot, 1);
+        TQ_CK(cudaMalloc(&base_, bytes));
+        step_ = reinterpret_cast<int*>(base_);
+        insts_ = reinterpret_cast<InstTask<T>*>(base_ + 256);
+        refs_ = reinterpret_cast<UpdRef*>(base_ + 256 + sizeof(InstTask<T>) * B);
+        std::vector<InstTask<T>> it;
+        for (int b = 0; b < B; ++b) it.push_back(eng_[b]->inst_task(step_, rows_cap_));
+        TQ_CK(cudaMemcpy(insts_, it.data(), sizeof(InstTask<T>) * B, cudaMemcpyHostToDevice));
+        if (nref_tot) TQ_CK(cudaMemcpy(refs_, refs.data(), sizeof(UpdRef) * nref_tot, cudaMemcpyHostToDevice));
+        for (auto& e : eng_) TQ_CK(cudaStreamSynchronize(e->own_stream()));
+    }
+    ~BatchEngine() {
+        if (st_) cudaStreamSynchronize(st_);
+        if (e0_) cudaEventDestroy(e0_);
+        if (e1_) cudaEventDestroy(e1_);
+        if (base_) cudaFree(base_);
+        if (st_) cudaStreamDestroy(st_);
+    }
+    int size() const { return (int)eng_.size(); }
+    Engine<T>& at(int b) { return *eng_[b]; }
+
+    void run(int k0, int k1) {
+        const int B = (int)eng_.size();
+        k_set_int<<<1, 1, 0, st_>>>(step_, k0);
+        TQ_CK(cudaGetLastError());
+        TQ_CK(cudaEventRecord(e0_, st_));
+        for (int k = k0; k < k1; ++k) {
+            launch_single_site_batch<T>(insts_, B, n_max_, cap_max_ * cap_max_, st_);
+            for (int q = 0; q < q_max_; ++q) {
+                const int nref = (int)(refs_off_[q + 1] - refs_off_[q]);
+                launch_update_batch<T>(insts_, refs_ + refs_off_[q], nref, cap_max_, 2 * cap_max_, block_, st_);
+                launches_ += 4;
+            }
+            launch_single_site_batch<T>(insts_, B, n_max_, cap_max_ * cap_max_, st_);
+            launch_entropy_batch<T>(insts_, B, st_);
+            launch_step_inc(step_, st_);
+            launches_ += 4;
+        }
+        TQ_CK(cudaEventRecord(e1_, st_));
+        TQ_CK(cudaStreamSynchronize(st_));
+        TQ_CK(cudaGetLastError());
+        float ms = 0;
+        TQ_CK(cudaEventElapsedTime(&ms, e0_, e1_));
+        ms_ = ms;
+    }
+    double ms() const { return ms_; }
+    long long launches() const { return launches_; }
+
+private:
+    std::vector<std::unique_ptr<Engine<T>>> eng_;
+    cudaStream_t st_ = nullptr;
+    cudaEvent_t e0_ = nullptr, e1_ = nullptr;
+    char* base_ = nullptr;
+    int* step_ = nullptr;
+    InstTask<T>* insts_ = nullptr;
+    UpdRef* refs_ = nullptr;
+    std::vector<size_t> refs_off_;
+    int cap_max_ = 1, n_max_ = 1, q_max_ = 0, steps_ = 0, block_ = 8, rows_cap_ = 8;
+    double ms_ = 0.0;
+    long long launches_ = 0;
+};
+
+template <typename T>
+static void run_batch(const std::vector<ProblemHost>& P, const std::vector<Config>& C,
+                      const tessera_qa_config* configs, tessera_qa_result* results) {
+    BatchEngine<T> be(P, C);
+    int k0 = (int)configs[0].step_begin;
+    int k1 = configs[0].step_end ? (int)configs[0].step_end : P[0].steps;
+    for (size_t b = 0; b < P.size(); ++b)
+        if (P[b].steps != P[0].steps) throw ArgError("batched instances must share the number of schedule steps");
+    if (k0 > k1 || k1 > P[0].steps) throw ArgError("step range outside the schedule");
+    be.run(k0, k1);
+    for (int b = 0; b < be.size(); ++b) {
+        Engine<T>& e = be.at(b);
+        tessera_qa_result r = results[b];
+        e.sync_stats(&r);
+        r.device_ms = be.ms();
+        r.kernel_launches = be.launches();
+        if (!configs[b].skip_observables) e.observe(&r);
+        if (r.entropy) e.copy_entropy(r.entropy, k0, k1);
+        if (r.final_mps) e.save(r.final_mps, r.final_mps_bytes, (unsigned long long)k1);
+        results[b] = r;
+    }
+}
+
 }  // namespace tq
 
 using namespace tq;
@@ -726,6 +879,36 @@ int tessera_qa_anneal_ex(const tessera_qa_problem* problem, const tessera_qa_con
         *result = r;
         if (r.status) {
             set_err("kernel status bits set: " + std::to_string(r.status));
+            return TESSERA_QA_ESTATUS;
+        }
+        return 0;
+    });
+}
+
+int tessera_qa_anneal_batch(const tessera_qa_problem* problems, const tessera_qa_config* configs,
+                            tessera_qa_result* results, size_t count) {
+    return guarded([&]() -> int {
+        if (!problems || !configs || !results) throw ArgError("problems, configs and results must be non-NULL");
+        if (count == 0) return 0;
+        std::vector<ProblemHost> P;
+        std::vector<Config> C;
+        for (size_t b = 0; b < count; ++b) {
+            P.push_back(validate_problem(&problems[b]));
+            C.push_back(validate_config(&configs[b]));
+            if (C.back().precision != C[0].precision) throw ArgError("batched instances must share the precision");
+            if (configs[b].initial_mps) throw ArgError("batched runs start from |+>^n");
+        }
+        if (C[0].device >= 0) TQ_CK(cudaSetDevice(C[0].device));
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw CudaError("no CUDA device available");
+        if (C[0].precision == TESSERA_QA_C64)
+            run_batch<float>(P, C, configs, results);
+        else
+            run_batch<double>(P, C, configs, results);
+        int st = 0;
+        for (size_t b = 0; b < count; ++b) st |= results[b].status;
+        if (st) {
+            set_err("kernel status bits set: " + std::to_string(st));
             return TESSERA_QA_ESTATUS;
         }
         return 0;

@@ -73,6 +73,45 @@ struct SvdWork {
     RunStats* stats;
 };
 
+struct SvdParams {
+    int bond;
+    int R, N;          // > 0: explicit matrix shape (standalone SVD); else 2*dims[bond], 2*dims[bond+2]
+    int no_trunc;      // 1: keep all min(R, N) values, leave dims and run statistics alone
+    int chi;
+    double tol;
+    double tiny;       // columns with |w|^2 below this are never rotated
+    int max_sweeps;
+    int rows_cap;      // shared-memory column length
+};
+
+struct ChainStep {
+    int site;
+    int zflag;
+    long long in_off;   // element offset of the input env in `envs`
+    long long out_off;  // element offset of the output env
+};
+
+// Per-instance views used by the batched kernels (one entry per instance).
+template <typename T>
+struct InstTask {
+    MpsView<T> mps;
+    ScheduleView sch;
+    SvdWork<T> wk;
+    SvdParams pp;              // bond is taken from the UpdRef
+    const ChainStep* ent_steps;
+    int n_ent;
+    int pad;
+    cplx_t<T>* envs;
+    cplx_t<T>* X;
+    long long r1_off;
+    double* entropy;
+};
+// One two-site update of one instance in a batched launch.
+struct UpdRef {
+    int inst;
+    GateOp op;
+};
+
 // ---- launchers (kernels.cu) ----
 template <typename T>
 void launch_single_site(const MpsView<T>& mps, const ScheduleView& sch, int dl_ub_max, cudaStream_t s);
@@ -91,12 +130,6 @@ void launch_absorb(const MpsView<T>& mps, int bond, SvdWork<T> wk, int rows_ub, 
 // site, optionally with Z inserted on that site's physical index:
 //   left : E'[b,b'] = sum_{a,a',s} E[a,a'] A(a,s,b) z_s conj(A(a',s,b'))
 //   right: E'[a,a'] = sum_{s,b,b'} A(a,s,b) E[b,b'] z_s conj(A(a',s,b'))
-struct ChainStep {
-    int site;
-    int zflag;
-    long long in_off;   // element offset of the input env in `envs`
-    long long out_off;  // element offset of the output env
-};
 template <typename T>
 void launch_chain(const MpsView<T>& mps, int right, const ChainStep* d_steps, int nsteps, cplx_t<T>* envs,
                   cplx_t<T>* scratch, GridBar* bar, RunStats* stats, int d_ub, cudaStream_t s);
@@ -117,6 +150,14 @@ template <typename T>
 void launch_amplitude(const MpsView<T>& mps, const int8_t* spins, cplx_t<T>* scratch, double* out_amp2,
                       cudaStream_t s);
 void launch_step_inc(int* step, cudaStream_t s);
+// batched launchers: `refs` selects (instance, gate) pairs; ub_* are upper bounds over the batch
+template <typename T>
+void launch_single_site_batch(const InstTask<T>* insts, int ninst, int n_max, int d2_ub_max, cudaStream_t s);
+template <typename T>
+void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref, int d_ub, int rows_ub,
+                         int block_w, cudaStream_t s);
+template <typename T>
+void launch_entropy_batch(const InstTask<T>* insts, int ninst, cudaStream_t s);
 template <typename T>
 void launch_init_plus(const MpsView<T>& mps, cudaStream_t s);
 

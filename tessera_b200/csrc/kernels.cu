@@ -73,9 +73,10 @@ void launch_step_inc(int* step, cudaStream_t s) {
 // cos(phi) I - i sin(phi) (nx X + nz Z)/r with r = |(nx, nz)|, phi = r dt/2.
 // ------------------------------------------------------------------------------------
 template <typename T>
-__global__ void k_single_site(MpsView<T> mps, ScheduleView sch) {
+__device__ __forceinline__ void single_site_body(const MpsView<T>& mps, const ScheduleView& sch, const int i,
+                                                 const int bx, const int nbx) {
     using V = cplx_t<T>;
-    const int i = blockIdx.y;
+    if (i >= mps.n) return;
     const int k = *sch.step;
     const double A = sch.sa[k], B = sch.sb[k];
     const double nx = -A, nz = -B * sch.h[i];
@@ -92,7 +93,7 @@ __global__ void k_single_site(MpsView<T> mps, ScheduleView sch) {
     const int dl = mps.dims[i], dr = mps.dims[i + 1];
     V* S = mps.site(i);
     const int tot = dl * dr;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += gridDim.x * blockDim.x) {
+    for (int t = bx * blockDim.x + threadIdx.x; t < tot; t += nbx * blockDim.x) {
         const int a = t / dr, b = t - a * dr;
         V* p0 = S + (long long)(2 * a) * mps.cap + b;
         V* p1 = p0 + mps.cap;
@@ -103,6 +104,11 @@ __global__ void k_single_site(MpsView<T> mps, ScheduleView sch) {
         *p0 = y0;
         *p1 = y1;
     }
+}
+
+template <typename T>
+__global__ void k_single_site(MpsView<T> mps, ScheduleView sch) {
+    single_site_body<T>(mps, sch, blockIdx.y, blockIdx.x, gridDim.x);
 }
 
 template <typename T>
@@ -140,14 +146,14 @@ __device__ __forceinline__ void gate_of(const GateOp& op, const ScheduleView& sc
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_theta(MpsView<T> mps, ScheduleView sch, GateOp op, const double* gen,
-                                               SvdWork<T> wk) {
+__device__ __forceinline__ void theta_tile(const MpsView<T>& mps, const ScheduleView& sch, const GateOp& op,
+                                           const double* gen, const SvdWork<T>& wk, const int tile_a, const int tile_b) {
     using V = cplx_t<T>;
     __shared__ V As[TH_KC][2][32];
     __shared__ V Cs[TH_KC][2][32];
     const int i = op.bond;
     const int dl = mps.dims[i], mid = mps.dims[i + 1], dr = mps.dims[i + 2];
-    const int a0 = blockIdx.x * 32, b0 = blockIdx.y * 32;
+    const int a0 = tile_a * 32, b0 = tile_b * 32;
     if (a0 >= dl || b0 >= dr) return;
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
     const V* A = mps.site(i);
@@ -216,6 +222,12 @@ __global__ void __launch_bounds__(256) k_theta(MpsView<T> mps, ScheduleView sch,
 }
 
 template <typename T>
+__global__ void __launch_bounds__(256) k_theta(MpsView<T> mps, ScheduleView sch, GateOp op, const double* gen,
+                                               SvdWork<T> wk) {
+    theta_tile<T>(mps, sch, op, gen, wk, blockIdx.x, blockIdx.y);
+}
+
+template <typename T>
 void launch_theta(const MpsView<T>& mps, const ScheduleView& sch, GateOp op, const double* gen_gate,
                   SvdWork<T> wk, int dl_ub, int dr_ub, cudaStream_t s) {
     dim3 grid((dl_ub + 31) / 32, (dr_ub + 31) / 32);
@@ -242,16 +254,6 @@ void launch_theta(const MpsView<T>& mps, const ScheduleView& sch, GateOp op, con
 // (keep = min(chi, k), then drop trailing sigma < 1e-14) and records the discarded
 // weight ratio.
 // ------------------------------------------------------------------------------------
-struct SvdParams {
-    int bond;
-    int R, N;          // > 0: explicit matrix shape (standalone SVD); else 2*dims[bond], 2*dims[bond+2]
-    int no_trunc;      // 1: keep all min(R, N) values, leave dims and run statistics alone
-    int chi;
-    double tol;
-    double tiny;       // columns with |w|^2 below this are never rotated
-    int max_sweeps;
-    int rows_cap;      // shared-memory column length
-};
 
 template <int G>
 __device__ __forceinline__ void group_reduce4(double v[4], double* red, int tid) {
@@ -318,6 +320,16 @@ __device__ __forceinline__ int rotate_pair(cplx_t<T>* cp, cplx_t<T>* cq, bool va
     return 1;
 }
 
+// Barrier across the CTAs that share one SVD: the grid barrier when several cooperate,
+// a plain CTA barrier when one CTA does it all.
+__device__ __forceinline__ bool cta_sync(GridBar* bar, int* status, unsigned int nblk) {
+    if (nblk == 1) {
+        __syncthreads();
+        return true;
+    }
+    return grid_sync(bar, status, nblk);
+}
+
 __device__ __forceinline__ void tournament(int P, int r, int pr, int& I, int& J) {
     const int Q = P - 1;
     if (pr == 0) {
@@ -342,13 +354,15 @@ struct SvdShape {
     static constexpr int NT = RPL > 0 ? 32 * BW : SVD_THREADS;
 };
 
+// Whole SVD of one theta by `ncta` cooperating CTAs (this one is number `cta`); with
+// ncta == 1 a single CTA runs every block pair itself and needs no grid barrier.
 template <typename T, int BW, int RPL>
-__global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdParams pp) {
+__device__ __forceinline__ void svd_body(const MpsView<T>& mps, const SvdWork<T>& wk, const SvdParams& pp,
+                                         const int cta, const int ncta, unsigned char* smraw) {
     using V = cplx_t<T>;
     constexpr int NT = SvdShape<BW, RPL>::NT;
     constexpr int NW = NT / 32;
     constexpr int G = NT / BW;
-    extern __shared__ __align__(16) unsigned char smraw[];
     V* col = reinterpret_cast<V*>(smraw);  // [2*BW][rows_cap]
     __shared__ double red[4 * NW];         // [warps][4]
     __shared__ int s_rot;
@@ -363,19 +377,24 @@ __global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd(MpsView<T> mps
     V* W = wk.W;
     const int nb = (N + BW - 1) / BW;
     const int P = nb + (nb & 1);
-    const unsigned int nblk = gridDim.x;
+    const unsigned int nblk = (unsigned)ncta;
     int* status = &wk.stats->status;
     if (R > pp.rows_cap) {  // host sizing bug guard: never index past shared memory
-        if (blockIdx.x == 0 && tid == 0) atomicOr(status, ST_BAD_DIMS);
+        if (cta == 0 && tid == 0) atomicOr(status, ST_BAD_DIMS);
         return;
     }
     const int grp = tid / G;
+    if (ncta == 1) {  // a lone CTA owns its counters (cooperative launches zero them on the host)
+        for (int e = tid; e < pp.max_sweeps; e += NT) wk.counters[e] = 0;
+        if (tid == 0) wk.scal[0] = 0.0;
+        __syncthreads();
+    }
     // ||W||_F^2 first: columns whose squared norm is below the noise floor of the matrix
     // (tiny) are never rotated, and the keep rule drops them.
     {
         const int warp = tid >> 5, lane = tid & 31;
         double part = 0.0;
-        for (int j = blockIdx.x * NW + warp; j < N; j += gridDim.x * NW) {
+        for (int j = cta * NW + warp; j < N; j += ncta * NW) {
             double sj = 0.0;
             const V* w = W + (long long)j * ld;
             for (int row = lane; row < R; row += 32) sj += (double)w[row].x * w[row].x + (double)w[row].y * w[row].y;
@@ -389,7 +408,7 @@ __global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd(MpsView<T> mps
             if (b != 0.0) atomicAdd(&wk.scal[0], b);
         }
     }
-    if (!grid_sync(wk.bar, status, nblk)) return;
+    if (!cta_sync(wk.bar, status, nblk)) return;
     const double fro2 = *(volatile double*)&wk.scal[0];
     // Noise floor: a column whose norm is below 8 sqrt(R) ulps of ||W||_F carries only rounding
     // noise; it is frozen (never rotated) and dropped by the keep rule.  Rotating such columns
@@ -402,7 +421,7 @@ __global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd(MpsView<T> mps
     bool converged = false;
     for (; sweep < pp.max_sweeps; ++sweep) {
         for (int r = 0; r < P - 1; ++r) {
-            for (int pr = blockIdx.x; pr < P / 2; pr += gridDim.x) {
+            for (int pr = cta; pr < P / 2; pr += ncta) {
                 int I, J;
                 tournament(P, r, pr, I, J);
                 // stage columns with 1-D TMA bulk copies: local c < BW -> block I, c >= BW -> block J
@@ -534,7 +553,7 @@ __global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd(MpsView<T> mps
                 if (tid == 0 && s_rot) atomicAdd(&wk.counters[sweep], s_rot);
                 __syncthreads();
             }
-            if (!grid_sync(wk.bar, status, nblk)) return;
+            if (!cta_sync(wk.bar, status, nblk)) return;
         }
         const int done = *(volatile int*)&wk.counters[sweep];
         if (done == 0) {
@@ -546,7 +565,7 @@ __global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd(MpsView<T> mps
     // column norms -> sig2 (FP64)
     {
         const int warp = tid >> 5, lane = tid & 31;
-        for (int j = blockIdx.x * NW + warp; j < N; j += gridDim.x * NW) {
+        for (int j = cta * NW + warp; j < N; j += ncta * NW) {
             double s = 0.0;
             const V* w = W + (long long)j * ld;
             for (int row = lane; row < R; row += 32) s += (double)w[row].x * w[row].x + (double)w[row].y * w[row].y;
@@ -554,8 +573,8 @@ __global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd(MpsView<T> mps
             if (lane == 0) wk.sig2[j] = s;
         }
     }
-    if (!grid_sync(wk.bar, status, nblk)) return;
-    if (blockIdx.x != 0) return;
+    if (!cta_sync(wk.bar, status, nblk)) return;
+    if (cta != 0) return;
     // ---- K3: sort + keep rule + discarded weight (CTA 0) ----
     double* key = reinterpret_cast<double*>(smraw);
     int* idx = reinterpret_cast<int*>(key + 4096);
@@ -644,6 +663,27 @@ __global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd(MpsView<T> mps
 }
 
 template <typename T, int BW, int RPL>
+__global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdParams pp) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    svd_body<T, BW, RPL>(mps, wk, pp, blockIdx.x, gridDim.x, smraw);
+}
+
+// Batched: each CTA takes whole SVD tasks (one theta each) in turn; no inter-CTA waits.
+template <typename T, int BW, int RPL>
+__global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd_batch(const InstTask<T>* insts, const UpdRef* refs,
+                                                                       int nref) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    for (int t = blockIdx.x; t < nref; t += gridDim.x) {
+        const UpdRef rf = refs[t];
+        const InstTask<T>& it = insts[rf.inst];
+        SvdParams pp = it.pp;
+        pp.bond = rf.op.bond;
+        svd_body<T, BW, RPL>(it.mps, it.wk, pp, 0, 1, smraw);
+        __syncthreads();
+    }
+}
+
+template <typename T, int BW, int RPL>
 static int svd_launch_bw(const MpsView<T>& mps, const SvdParams& pp, SvdWork<T> wk, int cols_ub,
                          cudaStream_t s) {
     using V = cplx_t<T>;
@@ -710,12 +750,12 @@ int launch_svd(const MpsView<T>& mps, int bond, int chi, double tol, int max_swe
 // C_new(k, s2, b) = (1/sigma_k) sum_row conj(W[row, perm[k]]) theta[row, s2*Dr + b].
 // ------------------------------------------------------------------------------------
 template <typename T>
-__global__ void k_absorb_u(MpsView<T> mps, int bond, SvdWork<T> wk) {
+__device__ __forceinline__ void absorb_u_tile(const MpsView<T>& mps, int bond, const SvdWork<T>& wk, int tk, int tr) {
     using V = cplx_t<T>;
     const int R = 2 * mps.dims[bond];
     const int keep = mps.dims[bond + 1];
-    const int k = blockIdx.x * 32 + threadIdx.x;
-    const int row = blockIdx.y * 8 + threadIdx.y;
+    const int k = tk * 32 + threadIdx.x;
+    const int row = tr * 8 + threadIdx.y;
     if (k >= keep || row >= R) return;
     const double inv = 1.0 / wk.sig[k];
     const V w = wk.W[(long long)wk.perm[k] * wk.ld + row];
@@ -723,7 +763,12 @@ __global__ void k_absorb_u(MpsView<T> mps, int bond, SvdWork<T> wk) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_absorb_c(MpsView<T> mps, int bond, SvdWork<T> wk) {
+__global__ void k_absorb_u(MpsView<T> mps, int bond, SvdWork<T> wk) {
+    absorb_u_tile<T>(mps, bond, wk, blockIdx.x, blockIdx.y);
+}
+
+template <typename T>
+__device__ __forceinline__ void absorb_c_tile(const MpsView<T>& mps, int bond, const SvdWork<T>& wk, int tc, int tk) {
     using V = cplx_t<T>;
     constexpr int KC = 8;
     __shared__ V Us[KC][32];
@@ -733,7 +778,7 @@ __global__ void __launch_bounds__(256) k_absorb_c(MpsView<T> mps, int bond, SvdW
     const int keep = mps.dims[bond + 1];
     const int dr = mps.dims[bond + 2];
     const int N = 2 * dr;
-    const int k0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    const int k0 = tk * 32, c0 = tc * 32;
     if (k0 >= keep || c0 >= N) return;
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
     if (tid < 32) pk[tid] = (k0 + tid < keep) ? wk.perm[k0 + tid] : -1;
@@ -777,6 +822,11 @@ __global__ void __launch_bounds__(256) k_absorb_c(MpsView<T> mps, int bond, SvdW
 }
 
 template <typename T>
+__global__ void __launch_bounds__(256) k_absorb_c(MpsView<T> mps, int bond, SvdWork<T> wk) {
+    absorb_c_tile<T>(mps, bond, wk, blockIdx.x, blockIdx.y);
+}
+
+template <typename T>
 void launch_absorb(const MpsView<T>& mps, int bond, SvdWork<T> wk, int rows_ub, int cols_ub, int keep_ub,
                    cudaStream_t s) {
     k_absorb_u<T><<<dim3((keep_ub + 31) / 32, (rows_ub + 7) / 8), dim3(32, 8), 0, s>>>(mps, bond, wk);
@@ -789,11 +839,11 @@ void launch_absorb(const MpsView<T>& mps, int bond, SvdWork<T> wk, int rows_ub, 
 // K6: environment transfer chain (cooperative; two GEMM phases per step).
 // ------------------------------------------------------------------------------------
 template <typename V, class LA, class LB, class ST>
-__device__ void gemm_phase(int M, int N, int K, LA la, LB lb, ST st, V (*As)[32], V (*Bs)[32]) {
+__device__ void gemm_phase(int M, int N, int K, LA la, LB lb, ST st, V (*As)[32], V (*Bs)[32], int cta, int ncta) {
     constexpr int KC = 8;
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
     const int tm = (M + 31) / 32, tn = (N + 31) / 32;
-    for (int t = blockIdx.x; t < tm * tn; t += gridDim.x) {
+    for (int t = cta; t < tm * tn; t += ncta) {
         const int i0 = (t / tn) * 32, j0 = (t % tn) * 32;
         V acc[2][2];
         for (int q = 0; q < 4; ++q) (&acc[0][0])[q] = czero<V>();
@@ -825,14 +875,14 @@ __device__ void gemm_phase(int M, int N, int K, LA la, LB lb, ST st, V (*As)[32]
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_chain(MpsView<T> mps, int right, const ChainStep* steps, int nsteps,
-                                               cplx_t<T>* envs, cplx_t<T>* X, GridBar* bar, RunStats* stats) {
+__device__ void chain_body(const MpsView<T>& mps, int right, const ChainStep* steps, int nsteps, cplx_t<T>* envs,
+                           cplx_t<T>* X, GridBar* bar, RunStats* stats, int cta, int ncta) {
     using V = cplx_t<T>;
     __shared__ V As[8][32];
     __shared__ V Bs[8][32];
     const int cap = mps.cap;
     const int ldx = 2 * cap;
-    const unsigned int nblk = gridDim.x;
+    const unsigned int nblk = (unsigned)ncta;
     for (int q = 0; q < nsteps; ++q) {
         const ChainStep cs = steps[q];
         const int dl = mps.dims[cs.site], dr = mps.dims[cs.site + 1];
@@ -850,13 +900,13 @@ __global__ void __launch_bounds__(256) k_chain(MpsView<T> mps, int right, const 
                     if (z && s) { v.x = -v.x; v.y = -v.y; }
                     return v;
                 },
-                [&](int i, int j, V v) { X[(long long)i * ldx + j] = v; }, As, Bs);
-            if (!grid_sync(bar, &stats->status, nblk)) return;
+                [&](int i, int j, V v) { X[(long long)i * ldx + j] = v; }, As, Bs, cta, ncta);
+            if (!cta_sync(bar, &stats->status, nblk)) return;
             // O[b, b'] = sum_{a', s} Y[a', s*dr + b] conj(A[(2a'+s), b'])
             gemm_phase<V>(dr, dr, 2 * dl,
                 [&](int i, int k) { return X[(long long)(k >> 1) * ldx + (k & 1) * dr + i]; },
                 [&](int k, int j) { V v = A[(long long)k * cap + j]; v.y = -v.y; return v; },
-                [&](int i, int j, V v) { O[(long long)i * cap + j] = v; }, As, Bs);
+                [&](int i, int j, V v) { O[(long long)i * cap + j] = v; }, As, Bs, cta, ncta);
         } else {
             // X[(2a+s), b'] = sum_b A[(2a+s), b] E[b, b'] z_s
             gemm_phase<V>(2 * dl, dr, dr,
@@ -866,8 +916,8 @@ __global__ void __launch_bounds__(256) k_chain(MpsView<T> mps, int right, const 
                     return v;
                 },
                 [&](int k, int j) { return E[(long long)k * cap + j]; },
-                [&](int i, int j, V v) { X[(long long)i * ldx + j] = v; }, As, Bs);
-            if (!grid_sync(bar, &stats->status, nblk)) return;
+                [&](int i, int j, V v) { X[(long long)i * ldx + j] = v; }, As, Bs, cta, ncta);
+            if (!cta_sync(bar, &stats->status, nblk)) return;
             // O[a, a'] = sum_{s, b'} X[(2a+s), b'] conj(A[(2a'+s), b'])   (k = s*dr + b')
             gemm_phase<V>(dl, dl, 2 * dr,
                 [&](int i, int k) {
@@ -880,10 +930,16 @@ __global__ void __launch_bounds__(256) k_chain(MpsView<T> mps, int right, const 
                     v.y = -v.y;
                     return v;
                 },
-                [&](int i, int j, V v) { O[(long long)i * cap + j] = v; }, As, Bs);
+                [&](int i, int j, V v) { O[(long long)i * cap + j] = v; }, As, Bs, cta, ncta);
         }
-        if (!grid_sync(bar, &stats->status, nblk)) return;
+        if (!cta_sync(bar, &stats->status, nblk)) return;
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_chain(MpsView<T> mps, int right, const ChainStep* steps, int nsteps,
+                                               cplx_t<T>* envs, cplx_t<T>* X, GridBar* bar, RunStats* stats) {
+    chain_body<T>(mps, right, steps, nsteps, envs, X, bar, stats, blockIdx.x, gridDim.x);
 }
 
 template <typename T>
@@ -908,7 +964,7 @@ void launch_chain(const MpsView<T>& mps, int right, const ChainStep* d_steps, in
 // with eigenvalues clamped to [0, 1] and terms lambda <= 1e-12 dropped
 // (cuda/src/mps.cpp:218-291).
 template <typename T>
-__global__ void k_entropy(MpsView<T> mps, const cplx_t<T>* r1, double* out, const int* step) {
+__device__ void entropy_body(const MpsView<T>& mps, const cplx_t<T>* r1, double* out, const int* step) {
     using V = cplx_t<T>;
     __shared__ double red[8][8];
     const int tid = threadIdx.x;
@@ -954,6 +1010,11 @@ __global__ void k_entropy(MpsView<T> mps, const cplx_t<T>* r1, double* out, cons
         }
         out[*step] = S;
     }
+}
+
+template <typename T>
+__global__ void k_entropy(MpsView<T> mps, const cplx_t<T>* r1, double* out, const int* step) {
+    entropy_body<T>(mps, r1, out, step);
 }
 
 template <typename T>
@@ -1029,6 +1090,113 @@ void launch_amplitude(const MpsView<T>& mps, const int8_t* spins, cplx_t<T>* scr
     TQ_CHECK(cudaGetLastError());
 }
 
+// ------------------------------------------------------------------------------------
+// Batched kernels: many instances (each with its own MPS, workspace and statistics) in
+// one launch.  Every instance keeps its own gate order; a launch runs gate q of every
+// instance that has one.
+// ------------------------------------------------------------------------------------
+template <typename T>
+__global__ void k_single_site_batch(const InstTask<T>* insts, int ninst) {
+    const InstTask<T>& it = insts[blockIdx.z];
+    single_site_body<T>(it.mps, it.sch, blockIdx.y, blockIdx.x, gridDim.x);
+}
+
+template <typename T>
+void launch_single_site_batch(const InstTask<T>* insts, int ninst, int n_max, int d2_ub_max, cudaStream_t s) {
+    int bx = (d2_ub_max + 255) / 256;
+    bx = bx < 1 ? 1 : (bx > 16 ? 16 : bx);
+    k_single_site_batch<T><<<dim3(bx, n_max, ninst), 256, 0, s>>>(insts, ninst);
+    TQ_CHECK(cudaGetLastError());
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_theta_batch(const InstTask<T>* insts, const UpdRef* refs) {
+    const UpdRef rf = refs[blockIdx.z];
+    const InstTask<T>& it = insts[rf.inst];
+    theta_tile<T>(it.mps, it.sch, rf.op, nullptr, it.wk, blockIdx.x, blockIdx.y);
+}
+
+template <typename T>
+__global__ void k_absorb_u_batch(const InstTask<T>* insts, const UpdRef* refs) {
+    const UpdRef rf = refs[blockIdx.z];
+    const InstTask<T>& it = insts[rf.inst];
+    absorb_u_tile<T>(it.mps, rf.op.bond, it.wk, blockIdx.x, blockIdx.y);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_absorb_c_batch(const InstTask<T>* insts, const UpdRef* refs) {
+    const UpdRef rf = refs[blockIdx.z];
+    const InstTask<T>& it = insts[rf.inst];
+    absorb_c_tile<T>(it.mps, rf.op.bond, it.wk, blockIdx.x, blockIdx.y);
+}
+
+template <typename T, int BW, int RPL>
+static void svd_batch_bw(const InstTask<T>* insts, const UpdRef* refs, int nref, int rows_cap, cudaStream_t s) {
+    using V = cplx_t<T>;
+    constexpr int NT = SvdShape<BW, RPL>::NT;
+    size_t smem = sizeof(V) * 2 * BW * (size_t)rows_cap;
+    const size_t sort_smem = 4096 * (sizeof(double) + sizeof(int));
+    if (smem < sort_smem) smem = sort_smem;
+    auto fn = k_svd_batch<T, BW, RPL>;
+    TQ_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    TQ_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, NT, smem));
+    if (per_sm < 1) throw std::runtime_error("k_svd_batch does not fit on an SM");
+    int grid = per_sm * num_sms();
+    if (grid > nref) grid = nref;
+    fn<<<grid, NT, smem, s>>>(insts, refs, nref);
+    TQ_CHECK(cudaGetLastError());
+}
+
+template <typename T>
+void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref, int d_ub, int rows_ub,
+                         int block_w, cudaStream_t s) {
+    if (nref <= 0) return;
+    const int tiles = (d_ub + 31) / 32;
+    k_theta_batch<T><<<dim3(tiles, tiles, nref), 256, 0, s>>>(insts, refs);
+    TQ_CHECK(cudaGetLastError());
+    const int rows_cap = ((rows_ub + 7) & ~7) < 8 ? 8 : ((rows_ub + 7) & ~7);
+    int rpl = 1;
+    while (32 * rpl < rows_cap) rpl <<= 1;
+    if (rpl > 16) throw std::runtime_error("batched SVD supports at most 512 rows");
+    int bw = block_w < 4 ? 4 : block_w;
+    if (rpl == 16 && bw > 8) bw = 8;
+#define TQ_RB(B, RP) \
+    if (bw == B && rpl == RP) { svd_batch_bw<T, B, RP>(insts, refs, nref, rows_cap, s); } else
+    TQ_RB(4, 1) TQ_RB(4, 2) TQ_RB(4, 4) TQ_RB(4, 8) TQ_RB(4, 16)
+    TQ_RB(8, 1) TQ_RB(8, 2) TQ_RB(8, 4) TQ_RB(8, 8) TQ_RB(8, 16)
+    TQ_RB(16, 1) TQ_RB(16, 2) TQ_RB(16, 4) TQ_RB(16, 8)
+    throw std::runtime_error("unsupported Jacobi block width");
+#undef TQ_RB
+    const int keep_tiles = (d_ub + 31) / 32;
+    k_absorb_u_batch<T><<<dim3(keep_tiles, (2 * d_ub + 7) / 8, nref), dim3(32, 8), 0, s>>>(insts, refs);
+    TQ_CHECK(cudaGetLastError());
+    k_absorb_c_batch<T><<<dim3((2 * d_ub + 31) / 32, keep_tiles, nref), 256, 0, s>>>(insts, refs);
+    TQ_CHECK(cudaGetLastError());
+}
+
+// One CTA per instance: right-environment chain to bond 1, then the qubit-0 entropy.
+template <typename T>
+__device__ void entropy_body(const MpsView<T>& mps, const cplx_t<T>* r1, double* out, const int* step);
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_entropy_batch(const InstTask<T>* insts) {
+    const InstTask<T>& it = insts[blockIdx.x];
+    if (it.mps.n >= 2) {
+        chain_body<T>(it.mps, 1, it.ent_steps, it.n_ent, it.envs, it.X, nullptr, it.wk.stats, 0, 1);
+        __syncthreads();
+        entropy_body<T>(it.mps, it.envs + it.r1_off, it.entropy, it.sch.step);
+    } else {
+        entropy_body<T>(it.mps, nullptr, it.entropy, it.sch.step);
+    }
+}
+
+template <typename T>
+void launch_entropy_batch(const InstTask<T>* insts, int ninst, cudaStream_t s) {
+    k_entropy_batch<T><<<ninst, 256, 0, s>>>(insts);
+    TQ_CHECK(cudaGetLastError());
+}
+
 // explicit instantiations
 #define TQ_INST(T)                                                                                          \
     template void launch_init_plus<T>(const MpsView<T>&, cudaStream_t);                                     \
@@ -1043,7 +1211,10 @@ void launch_amplitude(const MpsView<T>& mps, const int8_t* spins, cplx_t<T>* scr
     template void launch_entropy<T>(const MpsView<T>&, const cplx_t<T>*, double*, const int*, cudaStream_t); \
     template void launch_pair_dots<T>(const MpsView<T>&, const cplx_t<T>*, const PairDot*, int, double*,    \
                                       cudaStream_t);                                                        \
-    template void launch_amplitude<T>(const MpsView<T>&, const int8_t*, cplx_t<T>*, double*, cudaStream_t);
+    template void launch_amplitude<T>(const MpsView<T>&, const int8_t*, cplx_t<T>*, double*, cudaStream_t);   \
+    template void launch_single_site_batch<T>(const InstTask<T>*, int, int, int, cudaStream_t);                \
+    template void launch_update_batch<T>(const InstTask<T>*, const UpdRef*, int, int, int, int, cudaStream_t); \
+    template void launch_entropy_batch<T>(const InstTask<T>*, int, cudaStream_t);
 TQ_INST(double)
 TQ_INST(float)
 

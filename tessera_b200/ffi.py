@@ -306,3 +306,50 @@ class Session:
             self.close()
         except Exception:
             pass
+
+
+def anneal_batch(problems, dt=None, chi=None, precision="c128", zz_substeps=1, want_checkpoint=False,
+                 raise_on_status=True, skip_observables=False, jacobi_block=0, device=-1):
+    """tessera_qa_anneal_batch over a list of instances.Problem (each uses its own dt and chi unless
+    overridden); returns a list of AnnealResult in the same order."""
+    L = _lib.load()
+    B = len(problems)
+    P_arr = (_lib.Problem * B)()
+    C_arr = (_lib.Config * B)()
+    R_arr = (_lib.Result * B)()
+    keep = []
+    outs = []
+    for b, p in enumerate(problems):
+        Pb, kp = problem_struct(p.h, p.ei, p.ej, p.ew, p.sa, p.sb)
+        keep.append(kp)
+        P_arr[b] = Pb
+        cb, _ = config_struct(dt=dt if dt is not None else p.dt, chi=chi if chi is not None else p.chi,
+                              precision=precision, zz_substeps=zz_substeps, jacobi_block=jacobi_block,
+                              device=device, skip_observables=skip_observables)
+        C_arr[b] = cb
+        n, steps = p.n, p.steps
+        spins = np.zeros(n, np.int8)
+        zexp = np.zeros(n)
+        ent = np.zeros(max(steps, 1))
+        R_arr[b].spins = _p(spins, _lib.c_int8_p)
+        R_arr[b].z_expect = _p(zexp, _lib.c_double_p)
+        R_arr[b].entropy = _p(ent, _lib.c_double_p)
+        ck = None
+        if want_checkpoint:
+            nb = L.tessera_qa_checkpoint_bytes(n, cb.chi)
+            ck = np.zeros(nb, np.uint8)
+            R_arr[b].final_mps = ck.ctypes.data
+            R_arr[b].final_mps_bytes = nb
+        outs.append((spins, zexp, ent, ck, steps))
+    rc = L.tessera_qa_anneal_batch(P_arr, C_arr, R_arr, B)
+    if rc != 0 and not (rc == _lib.ESTATUS and not raise_on_status):
+        raise _lib.EngineError(rc, _lib.last_error())
+    res = []
+    for b in range(B):
+        spins, zexp, ent, ck, steps = outs[b]
+        r = R_arr[b]
+        res.append(AnnealResult(spins, r.energy, r.expected_energy, r.prob, r.max_trunc, r.norm2, ent[:steps],
+                                int(r.two_site_updates), int(r.status), int(r.max_sweeps), int(r.max_bond),
+                                float(r.device_ms), float(r.min_cut_gap), ck.tobytes() if ck is not None else None,
+                                zexp))
+    return res
