@@ -1,22 +1,27 @@
 #!/usr/bin/env python
 """Benchmark: TEBD two-site updates/s at chi=256.
 
-Workload (one instance per GPU, "replicas only": the anneal of one instance does not
-shard): n=128 chain with couplings to neighbours at distances 1..4, J ~ U(-1,1), h = 0,
-linear schedule, T=50, dt=0.02 (2500 steps), chi=256, complex128, the reference's gate
-order (each ZZ edge through the swap network: 1998 two-site updates per Trotter step).
-A bench step is one second-order Trotter step at mid-anneal (s = 0.5), run on a
-device-resident MPS whose every bond is at its cap min(256, 2^i, 2^(n-i)): the MPS starts
-as a seeded random state so that every timed update is a saturated chi=256 update.
+Workload: the n=128 chain with couplings to neighbours at distances 1..4 (J ~ U(-1,1), h = 0,
+linear schedule T=50, dt=0.02 -> 2500 steps), chi=256, complex128, each ZZ edge through the
+swap network in the reference's order (1998 two-site updates per Trotter step).  Every
+timed update is a saturated chi=256 update: each MPS starts as a seeded random state with
+every bond at its cap min(256, 2^i, 2^(n-i)).
+
+Default (--batch 148): 148 independent instances of that workload (seeds 2..149, one per
+SM) in one batched session; a bench step is 8 consecutive gate slots of the ZZ block of the
+Trotter step at s = 0.5 on every instance (148 x 8 two-site updates, each instance in its
+own reference gate order).  --batch 1 runs the plain single-instance engine, whose SVDs use
+all SMs cooperatively; its rate is also reported beside the batched line.
 
   python bench.py [--gpus N --steps K --warmup W]            # libtessera_qa.so
   python bench.py --impl reference [...]                     # the reference's CPU engine
 
 Printed: one JSON line on rank 0.  `value` = updates/s over all ranks with the MPS resident
 in HBM (CUDA events on the session stream, max over ranks); `e2e` = the same metric through
-the public C ABI tessera_qa_anneal_ex with host buffers (checkpoint in, checkpoint out);
-`roofline` = the Jacobi-SVD kernel's algorithmic bytes per launch over its average launch
-time; `cpu_baseline` = the reference engine timed on this host's cores.
+the host-buffer C ABI call tessera_qa_session_run_host (per step: h, J and the schedule
+copied from pinned host memory, run, statistics read back); `roofline` = the Jacobi-SVD
+kernel's algorithmic bytes per launch over its average launch time; `cpu_baseline` = the
+reference engine timed on this host's cores.
 """
 from __future__ import annotations
 
@@ -41,8 +46,10 @@ MID_STEP = 1250  # s = 1250/2499 ~ 0.5
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=148, help="instances per GPU (1 = plain single-instance engine)")
+    ap.add_argument("--gates", type=int, default=8, help="gate slots per bench step")
     ap.add_argument("--impl", choices=["tessera", "reference"], default="tessera")
     ap.add_argument("--precision", choices=["c128", "c64"], default="c128")
     ap.add_argument("--n", type=int, default=128)
@@ -192,15 +199,33 @@ def config_dict(args, p):
     return {"workload": f"chain n={args.n}, couplings at distances 1..{args.dmax}, J~U(-1,1), h=0, "
                         f"linear schedule T=50 dt=0.02, chi={args.chi}, one Trotter step at s=0.5",
             "n": args.n, "dmax": args.dmax, "chi": args.chi, "precision": args.precision,
-            "updates_per_step": p.updates_per_step(), "logical_zz_per_step": p.m,
+            "updates_per_trotter_step": p.updates_per_step(), "logical_zz_per_trotter_step": p.m,
             "gate_order": "reference (edges in order, swap network, truncation after every swap)",
             "l2": "inputs larger than L2 (MPS of 2*chi^2*16 B per site x n sites)",
-            "parallelism": "replicas" if args.gpus > 1 else "single GPU"}
+            "parallelism": "instance replicas (no data-path collective)"}
 
 
 # ------------------------------------------------------------------------------------
 # tessera engine
 # ------------------------------------------------------------------------------------
+def plain_rate(args, local):
+    """Plain single-instance engine (cooperative SVD over all SMs) on one instance, same gates."""
+    import torch
+
+    from tessera_b200 import ffi
+    p = workload(args, 0)
+    s = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=args.chi, precision=args.precision,
+                    kernel_timing=False, device=local)
+    s.randomize(1234)
+    s.run_gates(MID_STEP, 0, 2)
+    s.sync()
+    g = max(2, args.gates // 2)
+    s.run_gates(MID_STEP, 2, 2 + g)
+    r = s.sync()
+    s.close()
+    return g / (r.device_ms / 1e3), r.device_ms / g
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -219,18 +244,30 @@ def main():
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    p = workload(args, rank)
-    sess = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=args.chi, precision=args.precision,
-                       jacobi_block=args.jacobi_block, kernel_timing=True, device=local)
-    sess.randomize(1234 + rank)
-    upd_per_step = p.updates_per_step()
+    B = max(1, args.batch)
+    probs = [workload(args, rank * B + b) for b in range(B)]
+    p = probs[0]
+    upd_per_step_inst = min(args.gates, p.updates_per_step())
+    if B == 1:
+        sess = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=args.chi, precision=args.precision,
+                           jacobi_block=args.jacobi_block, kernel_timing=True, device=local)
+    else:
+        sess = ffi.Session.batch(probs, chi=args.chi, precision=args.precision, jacobi_block=args.jacobi_block,
+                                 kernel_timing=True, device=local)
+    sess.randomize(1234 + 1000 * rank)
+    G = upd_per_step_inst
+
+    def step(i):
+        q0 = (i * G) % (p.updates_per_step() - G + 1)
+        sess.run_gates(MID_STEP, q0, q0 + G)
+
     if args.profile_run:
-        sess.run(MID_STEP, 1)
+        step(0)
         r = sess.sync()
         print(f"profile run: {r.two_site_updates} updates, status {r.status}, {r.device_ms:.1f} ms")
         return
     for w in range(args.warmup):
-        sess.run(MID_STEP - args.warmup + w, 1)
+        step(w)
     r0 = sess.sync()
     stream = torch.cuda.ExternalStream(sess.stream)
     clocks = Clocks(local)
@@ -241,7 +278,8 @@ def main():
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    sess.run(MID_STEP, args.steps)
+    for k in range(args.steps):
+        step(args.warmup + k)
     e1.record(stream)
     r1 = sess.sync()
     torch.cuda.synchronize()
@@ -254,7 +292,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
     updates = r1.two_site_updates - r0.two_site_updates
-    assert updates == upd_per_step * args.steps, (updates, upd_per_step)
+    assert updates == B * G * args.steps, (updates, B, G)
     if r1.status:
         raise RuntimeError(f"engine status bits {r1.status} during the timed steps")
     value = updates * world / (ms_max / 1e3)
@@ -262,7 +300,7 @@ def main():
     svd_ms = r1.svd_ms - r0.svd_ms
     svd_bytes = r1.svd_bytes - r0.svd_bytes
     launches = r1.kernel_launches - r0.kernel_launches
-    sweeps = (r1.svd_sweeps - r0.svd_sweeps) / max(svd_n, 1)
+    sweeps = (r1.svd_sweeps - r0.svd_sweeps) / max(updates, 1)
     peak, peak_kind = peaks()
     achieved = (svd_bytes / svd_n) / (svd_ms / svd_n / 1e3) / 1e9 if svd_n else 0.0
     traffic = None
@@ -271,39 +309,51 @@ def main():
         try:
             with open(tf) as f:
                 d = json.load(f)
-            if d.get("chi") == args.chi and d.get("precision") == args.precision:
+            if d.get("chi") == args.chi and d.get("precision") == args.precision and d.get("batch") == B:
                 traffic = d.get("dram_bytes_per_launch")
         except Exception:
             traffic = None
-    roofline = {"kernel": "k_svd (one-sided Jacobi SVD of theta, 512 x 512)", "bound": "hbm",
-                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+    kname = "k_svd_batch (one CTA per 512x512 theta)" if B > 1 else "k_svd (cooperative, 512x512 theta)"
+    roofline = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak,
                 "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 "traffic": traffic, "avg_launch_ms": svd_ms / max(svd_n, 1),
                 "algorithmic_bytes_per_launch": svd_bytes / max(svd_n, 1), "avg_sweeps": sweeps,
                 "svd_share_of_step": svd_ms / ms if ms else None}
 
-    # ---- e2e through the public C ABI with host buffers ----
+    # ---- e2e: host-buffer ABI call per step (values from pinned host memory, stats back) ----
     e2e = None
     if not args.no_e2e:
-        ckpt = sess.save()  # current saturated state as a host checkpoint
-        pinned = torch.empty(len(ckpt), dtype=torch.uint8, pin_memory=True)
-        pinned.numpy()[:] = np.frombuffer(ckpt, np.uint8)
+        pinned = []
+        for q in probs:
+            cp = type(q)(*(torch.from_numpy(np.ascontiguousarray(x)).pin_memory().numpy()
+                           if isinstance(x, np.ndarray) else x for x in
+                           (q.h, q.ei, q.ej, q.ew, q.sa, q.sb, q.dt, q.chi, q.name)))
+            pinned.append(cp)
+        h2d = sum(q.h.nbytes + q.ew.nbytes + 2 * q.ei.nbytes + q.sa.nbytes + q.sb.nbytes for q in pinned)
         walls = []
-        h2d = len(ckpt) + p.h.nbytes + p.ew.nbytes + 2 * p.ei.nbytes + p.sa.nbytes + p.sb.nbytes
-        out = torch.empty(len(ckpt), dtype=torch.uint8, pin_memory=True)
-        d2h = len(ckpt) + 8 + 64  # final checkpoint (same dims), the step's entropy, result record
-        for k in range(1 + 1):  # one untimed call (allocation warm-up), one timed
+        for k in range(2):  # one untimed, one timed
+            q0 = (k * G) % (p.updates_per_step() - G + 1)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            ffi.anneal(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=args.chi, precision=args.precision,
-                       step_begin=MID_STEP + k, step_end=MID_STEP + k + 1, skip_observables=True,
-                       initial_mps=pinned.numpy(), checkpoint_out=out.numpy(), device=local,
-                       jacobi_block=args.jacobi_block)
-            torch.cuda.synchronize()
+            rr = sess.run_host(pinned, MID_STEP, q0, q0 + G)
             walls.append(time.perf_counter() - t0)
-        e2e = {"value": upd_per_step * world / walls[-1], "unit": UNIT, "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "api": "tessera_qa_anneal_ex (checkpoint in -> 1 Trotter step -> "
-                                                 "checkpoint out, host buffers)"}
+            if rr.status:
+                raise RuntimeError(f"engine status bits {rr.status} in the e2e step")
+        e2e = {"value": B * G * world / walls[-1], "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": 128 * B,
+               "api": "tessera_qa_session_run_host (h, J, schedule of every instance from pinned host memory -> "
+                      f"{G} gate slots -> run statistics to host)"}
+
+    plain = None
+    if B > 1 and rank == 0:
+        sess.close()
+        try:
+            pr, pms = plain_rate(args, local)
+            plain = {"value": pr, "unit": UNIT, "ms_per_update": pms,
+                     "engine": "plain single-instance, cooperative SVD across all SMs"}
+        except Exception as exc:
+            plain = {"value": None, "error": str(exc)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -318,17 +368,20 @@ def main():
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {exc}"}
 
     if rank == 0:
+        cfg = config_dict(args, p)
+        cfg.update({"instances_per_gpu": B, "gates_per_step": G,
+                    "step": f"{G} consecutive gate slots of the Trotter step at s=0.5 on each of {B} instances"})
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "c128" else "f32",
-                "data": "synthetic: seeded Ising instance (PCG64 seed 2+rank) and seeded random MPS with every "
+                "data": "synthetic: seeded Ising instances (PCG64 seeds 2..) and seeded random MPS with every "
                         "bond at its cap",
-                "config": config_dict(args, p), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": launches, "clocks": ck,
-                "logical_zz_gates_per_s": p.m * args.steps * world / (ms_max / 1e3),
+                "config": cfg, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches, "clocks": ck, "plain_single_instance": plain,
                 "max_trunc_in_timed_steps": r1.max_trunc}
         print(json.dumps(line))
-    sess.close()
+    if B == 1 or rank != 0:
+        sess.close()
     if world > 1:
         dist.destroy_process_group()
 

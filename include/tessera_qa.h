@@ -169,12 +169,27 @@ typedef struct tessera_qa_session tessera_qa_session;
 /* Uploads the problem and allocates the MPS at bond cap config->chi; state |+>^n. */
 TESSERA_QA_API tessera_qa_session* tessera_qa_session_create(const tessera_qa_problem* problem,
                                               const tessera_qa_config* config);
+/* A session over `count` independent instances run by the batched engine (see
+ * tessera_qa_anneal_batch); randomize / run / run_gates / run_host / sync apply to all of
+ * them (sync aggregates: summed updates, max discarded weight, ...). */
+TESSERA_QA_API tessera_qa_session* tessera_qa_session_create_batch(const tessera_qa_problem* problems,
+                                                                   const tessera_qa_config* configs, size_t count);
 /* Replaces the state by a seeded random MPS with every bond at its cap (min(chi, 2^i,
  * 2^(n-i))), sites scaled so theta stays O(1). */
 TESSERA_QA_API int tessera_qa_session_randomize(tessera_qa_session* s, uint64_t seed);
 /* Enqueues Trotter steps [step_begin, step_begin + nsteps) on the session's stream; returns
  * without waiting. */
 TESSERA_QA_API int tessera_qa_session_run(tessera_qa_session* s, size_t step_begin, size_t nsteps);
+/* Enqueues only gates [gate_begin, gate_end) of step `step`'s ZZ block (two-site updates in
+ * the reference's order; no single-site half steps, no entropy); returns without waiting. */
+TESSERA_QA_API int tessera_qa_session_run_gates(tessera_qa_session* s, size_t step, size_t gate_begin,
+                                                size_t gate_end);
+/* Host-buffer call: copies new h, J and schedule values from `problems` (host memory, one per
+ * instance, same n / edges / step count as at creation), runs step `step` (or only its gates
+ * [gate_begin, gate_end) when gate_end > 0), waits, and writes the run statistics to *result. */
+TESSERA_QA_API int tessera_qa_session_run_host(tessera_qa_session* s, const tessera_qa_problem* problems,
+                                               size_t count, size_t step, size_t gate_begin, size_t gate_end,
+                                               tessera_qa_result* result);
 /* The session's cudaStream_t. */
 TESSERA_QA_API void* tessera_qa_session_stream(tessera_qa_session* s);
 /* Waits for the stream and fills counters (updates, max_trunc, status, sweeps, bonds). */

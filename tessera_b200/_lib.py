@@ -85,6 +85,13 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.tessera_qa_last_error.restype = C.c_int
         L.tessera_qa_session_create.argtypes = [C.POINTER(Problem), C.POINTER(Config)]
         L.tessera_qa_session_create.restype = C.c_void_p
+        L.tessera_qa_session_create_batch.argtypes = [C.POINTER(Problem), C.POINTER(Config), C.c_size_t]
+        L.tessera_qa_session_create_batch.restype = C.c_void_p
+        L.tessera_qa_session_run_gates.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_size_t]
+        L.tessera_qa_session_run_gates.restype = C.c_int
+        L.tessera_qa_session_run_host.argtypes = [C.c_void_p, C.POINTER(Problem), C.c_size_t, C.c_size_t, C.c_size_t,
+                                                  C.c_size_t, C.POINTER(Result)]
+        L.tessera_qa_session_run_host.restype = C.c_int
         L.tessera_qa_session_randomize.argtypes = [C.c_void_p, C.c_uint64]
         L.tessera_qa_session_randomize.restype = C.c_int
         L.tessera_qa_session_run.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t]

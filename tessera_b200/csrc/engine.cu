@@ -157,6 +157,10 @@ public:
     virtual void init_plus() = 0;
     virtual void randomize(unsigned long long seed) = 0;
     virtual void run(int k0, int k1) = 0;
+    // gates [q0, q1) of the ZZ block of step k only (no single-site half steps, no entropy)
+    virtual void run_gates(int k, int q0, int q1) = 0;
+    // new values of h, J, A(s), B(s) for the same n, edges and number of steps
+    virtual void set_values(const ProblemHost& P) = 0;
     virtual void sync_stats(tessera_qa_result* r) = 0;
     virtual void observe(tessera_qa_result* r) = 0;
     virtual size_t save(void* buf, size_t bytes, unsigned long long step_next) = 0;
@@ -198,6 +202,7 @@ public:
         if (ev0_) cudaEventDestroy(ev0_);
         if (ev1_) cudaEventDestroy(ev1_);
         if (base_) cudaFree(base_);
+        if (obs_) cudaFree(obs_);
         if (stream_) cudaStreamDestroy(stream_);
     }
 
@@ -245,6 +250,29 @@ public:
         ran_ = true;
     }
 
+    void run_gates(int k, int q0, int q1) override {
+        if (k < 0 || k >= P_.steps || q0 < 0 || q1 > (int)ops_.size() || q0 > q1)
+            throw ArgError("gate range outside the step");
+        k_set_int<<<1, 1, 0, stream_>>>(step_, k);
+        TQ_CK(cudaGetLastError());
+        TQ_CK(cudaEventRecord(ev0_, stream_));
+        const ScheduleView sch = schedule();
+        const MpsView<T> M = mps();
+        for (int q = q0; q < q1; ++q) two_site(M, sch, ops_[q]);
+        TQ_CK(cudaEventRecord(ev1_, stream_));
+        ran_ = true;
+    }
+
+    void set_values(const ProblemHost& P) override {
+        if (P.n != n_ || P.m != m_ || P.steps != P_.steps || P.ei != P_.ei || P.ej != P_.ej)
+            throw ArgError("set_values needs the same n, edges and number of steps");
+        P_.h = P.h;
+        P_.w = P.w;
+        P_.sa = P.sa;
+        P_.sb = P.sb;
+        upload_problem();
+    }
+
     void sync_stats(tessera_qa_result* r) override {
         TQ_CK(cudaStreamSynchronize(stream_));
         TQ_CK(cudaGetLastError());
@@ -287,9 +315,16 @@ public:
     // <Z_i>, <Z_i Z_j>, <psi|psi>, readout, prob (cuda/src/mps.cpp:358-380).
     void observe(tessera_qa_result* r) override {
         const MpsView<T> M = mps();
-        launch_chain<T>(M, 1, obsR_, n_, envs_, xs_, bar_, stats_, cap_, stream_);
-        launch_chain<T>(M, 0, obsL_, n_obsL_, envs_, xs_, bar_, stats_, cap_, stream_);
-        launch_pair_dots<T>(M, envs_, dots_, 1 + n_ + m_, dotout_, stream_);
+        if (!obs_) {  // environments for the final observables, allocated on first use
+            const size_t bytes = sizeof(V) * (size_t)cap_ * cap_ * obs_units_;
+            TQ_CK(cudaMalloc(&obs_, bytes));
+            TQ_CK(cudaMemsetAsync(obs_, 0, sizeof(V), stream_));
+            V one = mk<V>(1, 0);
+            TQ_CK(cudaMemcpyAsync(obs_, &one, sizeof(V), cudaMemcpyHostToDevice, stream_));
+        }
+        launch_chain<T>(M, 1, obsR_, n_, obs_, xs_, bar_, stats_, cap_, stream_);
+        launch_chain<T>(M, 0, obsL_, n_obsL_, obs_, xs_, bar_, stats_, cap_, stream_);
+        launch_pair_dots<T>(M, obs_, dots_, 1 + n_ + m_, dotout_, stream_);
         std::vector<double> v(1 + n_ + m_);
         TQ_CK(cudaMemcpyAsync(v.data(), dotout_, sizeof(double) * v.size(), cudaMemcpyDeviceToHost, stream_));
         TQ_CK(cudaStreamSynchronize(stream_));
@@ -465,6 +500,8 @@ private:
     PairDot* dots_ = nullptr;
     int n_ent_ = 0, n_obsL_ = 0;
     long long r1_off_ = 0;
+    long long obs_units_ = 0;
+    V* obs_ = nullptr;
     std::vector<GateOp> ops_;
     std::vector<int> ub_;
     bool ran_ = false;
@@ -525,7 +562,7 @@ private:
     void allocate() {
         const size_t es = sizeof(V);
         const size_t unit = (size_t)cap_ * cap_;
-        const long long NE = 3 + 3LL * n_ + m_;
+        obs_units_ = 3 + 3LL * n_ + m_;  // observables: ONE, L_1..L_n, R_0..R_{n-1}, Z_i, ZZ_e, 2 temps
         // observable chain: L (n) + Z (n) + ZZ chains
         n_obsL_ = 2 * n_;
         for (int e = 0; e < m_; ++e) {
@@ -554,7 +591,7 @@ private:
         add((void**)&sb_, sizeof(double) * std::max(P_.steps, 1));
         add((void**)&step_, sizeof(int));
         add((void**)&entropy_, sizeof(double) * std::max(P_.steps, 1));
-        add((void**)&envs_, es * unit * NE);
+        add((void**)&envs_, es * unit * 3);  // entropy chain: ONE, two ping-pong buffers
         add((void**)&xs_, es * unit * 4);  // chain phase-1 product, up to (2 cap) x (2 cap)
         add((void**)&vbuf_, es * (size_t)2 * cap_);
         add((void**)&entc_, sizeof(ChainStep) * std::max(n_ent_, 1));
@@ -580,12 +617,13 @@ private:
         auto Zoff = [&](int i) { return (1LL + 2LL * n_ + i) * U; };
         auto ZZoff = [&](int e) { return (1LL + 3LL * n_ + e) * U; };
         const long long T0 = (1LL + 3LL * n_ + m_) * U, T1 = T0 + U;
+        const long long E0 = U, E1 = 2 * U;  // entropy ping-pong inside envs_
         std::vector<ChainStep> ent;
         for (int q = 0; q < n_ent_; ++q) {
             const int site = n_ - 1 - q;
-            ent.push_back(ChainStep{site, 0, q == 0 ? 0LL : ((q - 1) & 1 ? T1 : T0), (q & 1) ? T1 : T0});
+            ent.push_back(ChainStep{site, 0, q == 0 ? 0LL : ((q - 1) & 1 ? E1 : E0), (q & 1) ? E1 : E0});
         }
-        r1_off_ = n_ent_ ? (((n_ent_ - 1) & 1) ? T1 : T0) : 0;
+        r1_off_ = n_ent_ ? (((n_ent_ - 1) & 1) ? E1 : E0) : 0;
         std::vector<ChainStep> R, L;
         for (int q = 0; q < n_; ++q) {
             const int site = n_ - 1 - q;
@@ -692,8 +730,20 @@ static std::unique_ptr<EngineBase> make_engine(const ProblemHost& P, const Confi
 // one goes into one launch of each batched kernel (theta, one-CTA-per-task Jacobi SVD,
 // absorption), so each instance keeps the reference's gate order while the GPU is filled
 // with independent SVDs.
+class BatchBase {
+public:
+    virtual ~BatchBase() = default;
+    virtual int size() const = 0;
+    virtual void randomize(unsigned long long seed) = 0;
+    virtual void run(int k0, int k1) = 0;
+    virtual void run_gates(int k, int q0, int q1) = 0;
+    virtual void set_values(const std::vector<ProblemHost>& P) = 0;
+    virtual void sync(tessera_qa_result* r) = 0;  // aggregated over the instances
+    virtual cudaStream_t stream() const = 0;
+};
+
 template <typename T>
-class BatchEngine {
+class BatchEngine final : public BatchBase {
 public:
     BatchEngine(const std::vector<ProblemHost>& P, const std::vector<Config>& C) {
         const int B = (int)P.size();
@@ -733,42 +783,136 @@ public:
         if (nref_tot) TQ_CK(cudaMemcpy(refs_, refs.data(), sizeof(UpdRef) * nref_tot, cudaMemcpyHostToDevice));
         for (auto& e : eng_) TQ_CK(cudaStreamSynchronize(e->own_stream()));
     }
-    ~BatchEngine() {
+    ~BatchEngine() override {
         if (st_) cudaStreamSynchronize(st_);
+        for (cudaEvent_t e : pool_) cudaEventDestroy(e);
         if (e0_) cudaEventDestroy(e0_);
         if (e1_) cudaEventDestroy(e1_);
         if (base_) cudaFree(base_);
         if (st_) cudaStreamDestroy(st_);
     }
-    int size() const { return (int)eng_.size(); }
+    int size() const override { return (int)eng_.size(); }
     Engine<T>& at(int b) { return *eng_[b]; }
+    cudaStream_t stream() const override { return st_; }
+    void set_timing(bool on) { timing_ = on; }
 
-    void run(int k0, int k1) {
+    void randomize(unsigned long long seed) override {
+        for (size_t b = 0; b < eng_.size(); ++b) eng_[b]->randomize(seed + 7919ull * b);
+        for (auto& e : eng_) TQ_CK(cudaStreamSynchronize(e->own_stream()));
+    }
+
+    void set_values(const std::vector<ProblemHost>& P) override {
+        if (P.size() != eng_.size()) throw ArgError("set_values needs one problem per instance");
+        for (size_t b = 0; b < eng_.size(); ++b) eng_[b]->set_values(P[b]);
+    }
+
+    void run_gates(int k, int q0, int q1) override {
+        if (q0 < 0 || q1 > q_max_ || q0 > q1) throw ArgError("gate range outside the step");
+        k_set_int<<<1, 1, 0, st_>>>(step_, k);
+        TQ_CK(cudaGetLastError());
+        TQ_CK(cudaEventRecord(e0_, st_));
+        for (int q = q0; q < q1; ++q) slot(q);
+        TQ_CK(cudaEventRecord(e1_, st_));
+        ran_ = true;
+    }
+
+    void sync(tessera_qa_result* r) override {
+        TQ_CK(cudaStreamSynchronize(st_));
+        TQ_CK(cudaGetLastError());
+        if (ran_) {
+            float ms = 0;
+            TQ_CK(cudaEventElapsedTime(&ms, e0_, e1_));
+            ms_ = ms;
+            ran_ = false;
+        }
+        for (auto& pr : timed_) {
+            float ms = 0;
+            TQ_CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+            svd_ms_ += ms;
+        }
+        timed_.clear();
+        pool_next_ = 0;
+        if (!r) return;
+        tessera_qa_result a;
+        std::memset(&a, 0, sizeof(a));
+        a.min_cut_gap = 1.0;
+        for (auto& e : eng_) {
+            tessera_qa_result x;
+            std::memset(&x, 0, sizeof(x));
+            e->sync_stats(&x);
+            a.two_site_updates += x.two_site_updates;
+            a.max_trunc = std::max(a.max_trunc, x.max_trunc);
+            a.status |= x.status;
+            a.max_sweeps = std::max(a.max_sweeps, x.max_sweeps);
+            a.max_bond = std::max(a.max_bond, x.max_bond);
+            a.min_cut_gap = std::min(a.min_cut_gap, x.min_cut_gap);
+            a.svd_bytes += x.svd_bytes;
+            a.svd_sweeps += x.svd_sweeps;
+        }
+        r->two_site_updates = a.two_site_updates;
+        r->max_trunc = a.max_trunc;
+        r->status = a.status;
+        r->max_sweeps = a.max_sweeps;
+        r->max_bond = a.max_bond;
+        r->min_cut_gap = a.min_cut_gap;
+        r->svd_bytes = a.svd_bytes;
+        r->svd_sweeps = a.svd_sweeps;
+        r->svd_ms = svd_ms_;
+        r->svd_launches = svd_launches_;
+        r->kernel_launches = launches_;
+        r->device_ms = ms_;
+    }
+
+    void run(int k0, int k1) override {
         const int B = (int)eng_.size();
         k_set_int<<<1, 1, 0, st_>>>(step_, k0);
         TQ_CK(cudaGetLastError());
         TQ_CK(cudaEventRecord(e0_, st_));
         for (int k = k0; k < k1; ++k) {
             launch_single_site_batch<T>(insts_, B, n_max_, cap_max_ * cap_max_, st_);
-            for (int q = 0; q < q_max_; ++q) {
-                const int nref = (int)(refs_off_[q + 1] - refs_off_[q]);
-                launch_update_batch<T>(insts_, refs_ + refs_off_[q], nref, cap_max_, 2 * cap_max_, block_, st_);
-                launches_ += 4;
-            }
+            for (int q = 0; q < q_max_; ++q) slot(q);
             launch_single_site_batch<T>(insts_, B, n_max_, cap_max_ * cap_max_, st_);
             launch_entropy_batch<T>(insts_, B, st_);
             launch_step_inc(step_, st_);
             launches_ += 4;
         }
         TQ_CK(cudaEventRecord(e1_, st_));
-        TQ_CK(cudaStreamSynchronize(st_));
-        TQ_CK(cudaGetLastError());
-        float ms = 0;
-        TQ_CK(cudaEventElapsedTime(&ms, e0_, e1_));
-        ms_ = ms;
+        ran_ = true;
+        sync(nullptr);
     }
     double ms() const { return ms_; }
     long long launches() const { return launches_; }
+
+private:
+    // gate slot q of every instance that has one: theta, Jacobi SVD, absorption
+    void slot(int q) {
+        const int nref = (int)(refs_off_[q + 1] - refs_off_[q]);
+        cudaEvent_t a = nullptr, b = nullptr;
+        if (timing_) {
+            a = event();
+            b = event();
+        }
+        launch_update_batch<T>(insts_, refs_ + refs_off_[q], nref, cap_max_, 2 * cap_max_, block_, st_, a, b);
+        if (timing_) timed_.push_back({a, b});
+        launches_ += 4;
+        ++svd_launches_;
+    }
+    cudaEvent_t event() {
+        if (pool_next_ < pool_.size()) return pool_[pool_next_++];
+        cudaEvent_t e;
+        TQ_CK(cudaEventCreate(&e));
+        pool_.push_back(e);
+        ++pool_next_;
+        return e;
+    }
+    bool timing_ = false, ran_ = false;
+    double svd_ms_ = 0.0;
+    long long svd_launches_ = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timed_;
+    std::vector<cudaEvent_t> pool_;
+    size_t pool_next_ = 0;
+
+public:
 
 private:
     std::vector<std::unique_ptr<Engine<T>>> eng_;
@@ -812,9 +956,11 @@ static void run_batch(const std::vector<ProblemHost>& P, const std::vector<Confi
 using namespace tq;
 
 struct tessera_qa_session {
-    std::unique_ptr<EngineBase> eng;
+    std::unique_ptr<EngineBase> eng;     // single instance
+    std::unique_ptr<BatchBase> batch;    // or a batch of instances
     ProblemHost P;
     Config C;
+    std::vector<ProblemHost> PB;
 };
 
 template <typename F>
@@ -1010,10 +1156,43 @@ tessera_qa_session* tessera_qa_session_create(const tessera_qa_problem* problem,
     return rc == 0 ? out : nullptr;
 }
 
+tessera_qa_session* tessera_qa_session_create_batch(const tessera_qa_problem* problems,
+                                                    const tessera_qa_config* configs, size_t count) {
+    tessera_qa_session* out = nullptr;
+    const int rc = guarded([&]() -> int {
+        if (!problems || !configs || count == 0) throw ArgError("problems/configs must be non-NULL, count >= 1");
+        std::unique_ptr<tessera_qa_session> s(new tessera_qa_session);
+        std::vector<Config> C;
+        for (size_t b = 0; b < count; ++b) {
+            s->PB.push_back(validate_problem(&problems[b]));
+            C.push_back(validate_config(&configs[b]));
+            if (C.back().precision != C[0].precision) throw ArgError("batched instances must share the precision");
+            if (s->PB.back().steps != s->PB[0].steps) throw ArgError("batched instances must share the step count");
+        }
+        if (C[0].device >= 0) TQ_CK(cudaSetDevice(C[0].device));
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw CudaError("no CUDA device available");
+        s->C = C[0];
+        if (C[0].precision == TESSERA_QA_C64) {
+            auto* b = new BatchEngine<float>(s->PB, C);
+            b->set_timing(C[0].timing);
+            s->batch.reset(b);
+        } else {
+            auto* b = new BatchEngine<double>(s->PB, C);
+            b->set_timing(C[0].timing);
+            s->batch.reset(b);
+        }
+        out = s.release();
+        return 0;
+    });
+    return rc == 0 ? out : nullptr;
+}
+
 int tessera_qa_session_randomize(tessera_qa_session* s, uint64_t seed) {
     return guarded([&]() -> int {
         if (!s) throw ArgError("session is NULL");
-        s->eng->randomize(seed);
+        if (s->batch) s->batch->randomize(seed);
+        else s->eng->randomize(seed);
         return 0;
     });
 }
@@ -1021,19 +1200,56 @@ int tessera_qa_session_randomize(tessera_qa_session* s, uint64_t seed) {
 int tessera_qa_session_run(tessera_qa_session* s, size_t step_begin, size_t nsteps) {
     return guarded([&]() -> int {
         if (!s) throw ArgError("session is NULL");
-        s->eng->run((int)step_begin, (int)(step_begin + nsteps));
+        if (s->batch) s->batch->run((int)step_begin, (int)(step_begin + nsteps));
+        else s->eng->run((int)step_begin, (int)(step_begin + nsteps));
         return 0;
     });
 }
 
-void* tessera_qa_session_stream(tessera_qa_session* s) { return s ? (void*)s->eng->stream() : nullptr; }
+int tessera_qa_session_run_gates(tessera_qa_session* s, size_t step, size_t gate_begin, size_t gate_end) {
+    return guarded([&]() -> int {
+        if (!s) throw ArgError("session is NULL");
+        if (s->batch) s->batch->run_gates((int)step, (int)gate_begin, (int)gate_end);
+        else s->eng->run_gates((int)step, (int)gate_begin, (int)gate_end);
+        return 0;
+    });
+}
+
+int tessera_qa_session_run_host(tessera_qa_session* s, const tessera_qa_problem* problems, size_t count, size_t step,
+                                size_t gate_begin, size_t gate_end, tessera_qa_result* result) {
+    return guarded([&]() -> int {
+        if (!s || !problems) throw ArgError("session and problems must be non-NULL");
+        const size_t B = s->batch ? (size_t)s->batch->size() : 1;
+        if (count != B) throw ArgError("one problem per session instance is required");
+        std::vector<ProblemHost> P;
+        for (size_t b = 0; b < count; ++b) P.push_back(validate_problem(&problems[b]));
+        if (s->batch) {
+            s->batch->set_values(P);
+            if (gate_end) s->batch->run_gates((int)step, (int)gate_begin, (int)gate_end);
+            else s->batch->run((int)step, (int)step + 1);
+            s->batch->sync(result);
+        } else {
+            s->eng->set_values(P[0]);
+            if (gate_end) s->eng->run_gates((int)step, (int)gate_begin, (int)gate_end);
+            else s->eng->run((int)step, (int)step + 1);
+            s->eng->sync_stats(result);
+        }
+        return 0;
+    });
+}
+
+void* tessera_qa_session_stream(tessera_qa_session* s) {
+    if (!s) return nullptr;
+    return s->batch ? (void*)s->batch->stream() : (void*)s->eng->stream();
+}
 
 int tessera_qa_session_sync(tessera_qa_session* s, tessera_qa_result* result) {
     return guarded([&]() -> int {
         if (!s) throw ArgError("session is NULL");
         tessera_qa_result r;
         std::memset(&r, 0, sizeof(r));
-        s->eng->sync_stats(&r);
+        if (s->batch) s->batch->sync(&r);
+        else s->eng->sync_stats(&r);
         if (result) {
             result->max_trunc = r.max_trunc;
             result->two_site_updates = r.two_site_updates;
@@ -1055,6 +1271,7 @@ int tessera_qa_session_sync(tessera_qa_session* s, tessera_qa_result* result) {
 int tessera_qa_session_observe(tessera_qa_session* s, tessera_qa_result* result) {
     return guarded([&]() -> int {
         if (!s || !result) throw ArgError("session or result is NULL");
+        if (s->batch) throw ArgError("observe is per instance: use tessera_qa_anneal_batch for batched results");
         s->eng->sync_stats(result);
         s->eng->observe(result);
         return 0;
@@ -1064,6 +1281,7 @@ int tessera_qa_session_observe(tessera_qa_session* s, tessera_qa_result* result)
 int tessera_qa_session_save(tessera_qa_session* s, void* buf, size_t bytes) {
     return guarded([&]() -> int {
         if (!s) throw ArgError("session is NULL");
+        if (s->batch) throw ArgError("checkpoints are per instance");
         s->eng->save(buf, bytes, 0);
         return 0;
     });
@@ -1072,6 +1290,7 @@ int tessera_qa_session_save(tessera_qa_session* s, void* buf, size_t bytes) {
 int tessera_qa_session_load(tessera_qa_session* s, const void* buf, size_t bytes) {
     return guarded([&]() -> int {
         if (!s) throw ArgError("session is NULL");
+        if (s->batch) throw ArgError("checkpoints are per instance");
         s->eng->load(buf, bytes);
         return 0;
     });

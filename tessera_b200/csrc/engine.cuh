@@ -155,7 +155,8 @@ template <typename T>
 void launch_single_site_batch(const InstTask<T>* insts, int ninst, int n_max, int d2_ub_max, cudaStream_t s);
 template <typename T>
 void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref, int d_ub, int rows_ub,
-                         int block_w, cudaStream_t s);
+                         int block_w, cudaStream_t s, cudaEvent_t svd_begin = nullptr,
+                         cudaEvent_t svd_end = nullptr);
 template <typename T>
 void launch_entropy_batch(const InstTask<T>* insts, int ninst, cudaStream_t s);
 template <typename T>

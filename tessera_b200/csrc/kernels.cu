@@ -1150,7 +1150,7 @@ static void svd_batch_bw(const InstTask<T>* insts, const UpdRef* refs, int nref,
 
 template <typename T>
 void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref, int d_ub, int rows_ub,
-                         int block_w, cudaStream_t s) {
+                         int block_w, cudaStream_t s, cudaEvent_t svd_begin, cudaEvent_t svd_end) {
     if (nref <= 0) return;
     const int tiles = (d_ub + 31) / 32;
     k_theta_batch<T><<<dim3(tiles, tiles, nref), 256, 0, s>>>(insts, refs);
@@ -1161,6 +1161,7 @@ void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref,
     if (rpl > 16) throw std::runtime_error("batched SVD supports at most 512 rows");
     int bw = block_w < 4 ? 4 : block_w;
     if (rpl == 16 && bw > 8) bw = 8;
+    if (svd_begin) TQ_CHECK(cudaEventRecord(svd_begin, s));
 #define TQ_RB(B, RP) \
     if (bw == B && rpl == RP) { svd_batch_bw<T, B, RP>(insts, refs, nref, rows_cap, s); } else
     TQ_RB(4, 1) TQ_RB(4, 2) TQ_RB(4, 4) TQ_RB(4, 8) TQ_RB(4, 16)
@@ -1168,6 +1169,7 @@ void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref,
     TQ_RB(16, 1) TQ_RB(16, 2) TQ_RB(16, 4) TQ_RB(16, 8)
     throw std::runtime_error("unsupported Jacobi block width");
 #undef TQ_RB
+    if (svd_end) TQ_CHECK(cudaEventRecord(svd_end, s));
     const int keep_tiles = (d_ub + 31) / 32;
     k_absorb_u_batch<T><<<dim3(keep_tiles, (2 * d_ub + 7) / 8, nref), dim3(32, 8), 0, s>>>(insts, refs);
     TQ_CHECK(cudaGetLastError());
@@ -1213,7 +1215,8 @@ void launch_entropy_batch(const InstTask<T>* insts, int ninst, cudaStream_t s) {
                                       cudaStream_t);                                                        \
     template void launch_amplitude<T>(const MpsView<T>&, const int8_t*, cplx_t<T>*, double*, cudaStream_t);   \
     template void launch_single_site_batch<T>(const InstTask<T>*, int, int, int, cudaStream_t);                \
-    template void launch_update_batch<T>(const InstTask<T>*, const UpdRef*, int, int, int, int, cudaStream_t); \
+    template void launch_update_batch<T>(const InstTask<T>*, const UpdRef*, int, int, int, int, cudaStream_t,  \
+                                         cudaEvent_t, cudaEvent_t);                                          \
     template void launch_entropy_batch<T>(const InstTask<T>*, int, cudaStream_t);
 TQ_INST(double)
 TQ_INST(float)

@@ -245,7 +245,10 @@ def sites_to_dense(sites) -> np.ndarray:
 
 
 class Session:
-    """A device-resident anneal (tessera_qa_session_*): the MPS stays in HBM between calls."""
+    """A device-resident anneal (tessera_qa_session_*): the MPS stays in HBM between calls.
+
+    Session(h, ei, ej, ew, sa, sb, ...) holds one instance; Session.batch([problems], ...) holds
+    many, run by the batched engine."""
 
     def __init__(self, h, ei, ej, ew, sa, sb, dt=0.1, chi=32, precision="c128", zz_substeps=1,
                  kernel_timing=False, **kw):
@@ -256,9 +259,52 @@ class Session:
         c.kernel_timing = 1 if kernel_timing else 0
         self.chi = chi
         self.n = int(self._P.n)
+        self.count = 1
         self._h = L.tessera_qa_session_create(C.byref(self._P), C.byref(c))
         if not self._h:
             raise _lib.EngineError(_lib.ECUDA, _lib.last_error())
+
+    @classmethod
+    def batch(cls, problems, dt=None, chi=None, precision="c128", kernel_timing=False, **kw):
+        self = cls.__new__(cls)
+        L = _lib.load()
+        self._L = L
+        B = len(problems)
+        self._Parr = (_lib.Problem * B)()
+        Carr = (_lib.Config * B)()
+        self._keep = []
+        for b, p in enumerate(problems):
+            Pb, kp = problem_struct(p.h, p.ei, p.ej, p.ew, p.sa, p.sb)
+            self._keep.append(kp)
+            self._Parr[b] = Pb
+            cb, _ = config_struct(dt=dt if dt is not None else p.dt, chi=chi if chi is not None else p.chi,
+                                  precision=precision, **kw)
+            cb.kernel_timing = 1 if kernel_timing else 0
+            Carr[b] = cb
+        self.chi = chi
+        self.n = problems[0].n
+        self.count = B
+        self._h = L.tessera_qa_session_create_batch(self._Parr, Carr, B)
+        if not self._h:
+            raise _lib.EngineError(_lib.ECUDA, _lib.last_error())
+        return self
+
+    def run_gates(self, step: int, gate_begin: int, gate_end: int):
+        self._ck(self._L.tessera_qa_session_run_gates(self._h, step, gate_begin, gate_end))
+
+    def run_host(self, problems, step: int, gate_begin: int = 0, gate_end: int = 0) -> "_lib.Result":
+        """Host-buffer call: new h/J/schedule values from `problems` (host numpy arrays), run, wait,
+        return the run statistics."""
+        B = len(problems)
+        Parr = (_lib.Problem * B)()
+        keep = []
+        for b, p in enumerate(problems):
+            Pb, kp = problem_struct(p.h, p.ei, p.ej, p.ew, p.sa, p.sb)
+            keep.append(kp)
+            Parr[b] = Pb
+        r = _lib.Result()
+        self._ck(self._L.tessera_qa_session_run_host(self._h, Parr, B, step, gate_begin, gate_end, C.byref(r)))
+        return r
 
     def _ck(self, rc):
         if rc != 0:

@@ -241,3 +241,26 @@ def test_batched_anneal_equals_single_instance_runs():
             assert np.max(np.abs(rb.entropy - rs.entropy)) < tol * 10, (p.name, prec)
             assert spins_agree(rb, rs.spins)
             assert rb.status == 0
+
+
+def test_batch_session_gate_slots_match_single_sessions():
+    """Batched session (resident MPS of several instances, random saturated start): a run of gate
+    slots updates every instance exactly like a single-instance session does."""
+    probs = [instances.chain_range(n=12, dmax=3, seed=s, T=1.0, dt=0.05, chi=16) for s in (1, 2, 3)]
+    sb = ffi.Session.batch(probs, chi=16, kernel_timing=True)
+    sb.randomize(5)
+    sb.run_gates(3, 0, 10)
+    rb = sb.sync()
+    assert rb.two_site_updates == 30 and rb.status == 0 and rb.svd_launches == 10
+    tr = []
+    for b, p in enumerate(probs):
+        s1 = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=16)
+        s1.randomize(5 + 7919 * b)
+        s1.run_gates(3, 0, 10)
+        r1 = s1.sync()
+        tr.append(r1.max_trunc)
+        s1.close()
+    assert rb.max_trunc == pytest.approx(max(tr), rel=1e-9)
+    r2 = sb.run_host(probs, 4, 0, 5)
+    assert r2.status == 0
+    sb.close()
