@@ -217,10 +217,11 @@ def plain_rate(args, local):
     s = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=args.chi, precision=args.precision,
                     kernel_timing=False, device=local)
     s.randomize(1234)
-    s.run_gates(MID_STEP, 0, 2)
+    lo = 16 * min(32, args.n // 4)
+    s.run_gates(MID_STEP, lo, lo + 2)
     s.sync()
     g = max(2, args.gates // 2)
-    s.run_gates(MID_STEP, 2, 2 + g)
+    s.run_gates(MID_STEP, lo + 2, lo + 2 + g)
     r = s.sync()
     s.close()
     return g / (r.device_ms / 1e3), r.device_ms / g
@@ -256,10 +257,18 @@ def main():
                                  kernel_timing=True, device=local)
     sess.randomize(1234 + 1000 * rank)
     G = upd_per_step_inst
+    # Gate slots of edges (i, i+d) with 32 <= i < 96: every bond they touch sits at chi = 256
+    # (the chain's bond i is capped by 2^min(i, n-i)); each edge i owns 16 consecutive slots.
+    lo = 16 * min(32, args.n // 4)
+    span = max(G, 16 * (args.n // 2))
+
+    def window(i):
+        q0 = lo + (i * G) % max(1, span - G + 1)
+        return q0, min(q0 + G, p.updates_per_step())
 
     def step(i):
-        q0 = (i * G) % (p.updates_per_step() - G + 1)
-        sess.run_gates(MID_STEP, q0, q0 + G)
+        q0, q1 = window(i)
+        sess.run_gates(MID_STEP, q0, q1)
 
     if args.profile_run:
         step(0)
@@ -333,10 +342,10 @@ def main():
         h2d = sum(q.h.nbytes + q.ew.nbytes + 2 * q.ei.nbytes + q.sa.nbytes + q.sb.nbytes for q in pinned)
         walls = []
         for k in range(2):  # one untimed, one timed
-            q0 = (k * G) % (p.updates_per_step() - G + 1)
+            q0, q1 = window(args.warmup + args.steps + k)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            rr = sess.run_host(pinned, MID_STEP, q0, q0 + G)
+            rr = sess.run_host(pinned, MID_STEP, q0, q1)
             walls.append(time.perf_counter() - t0)
             if rr.status:
                 raise RuntimeError(f"engine status bits {rr.status} in the e2e step")
