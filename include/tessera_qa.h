@@ -71,6 +71,11 @@ typedef struct tessera_qa_problem {
     size_t steps;
     const double* schedule_a;
     const double* schedule_b;
+    /* Optional warm-start bias (NULL = none; not in the reference): a longitudinal field
+     * -C(s_k) sum_i bias_i Z_i added to H for step k, with C(s_k) = schedule_c[k].  Choosing
+     * C = 0 at both ends leaves the initial and final Hamiltonians unchanged. */
+    const double* bias;
+    const double* schedule_c;
 } tessera_qa_problem;
 
 typedef struct tessera_qa_config {

@@ -97,6 +97,8 @@ class Oracle:
                                      C.c_double, C.c_int, C.c_int, _i8p, _dp, _dp, _dp, C.c_int]
         L.orc_sv_anneal.argtypes = [_dp, C.c_int, _ip, _ip, _dp, C.c_int, _dp, _dp, C.c_int,
                                     C.c_double, C.c_int, _i8p, _i8p, _dp, _dp, _dp]
+        L.orc_sv_anneal_bias.argtypes = [_dp, C.c_int, _ip, _ip, _dp, C.c_int, _dp, _dp, C.c_int,
+                                         C.c_double, C.c_int, _i8p, _i8p, _dp, _dp, _dp, _dp, _dp]
         L.orc_exact_ground.argtypes = [_dp, C.c_int, _ip, _ip, _dp, C.c_int, _i8p]
         L.orc_exact_ground.restype = C.c_double
         L.orc_svd.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp]
@@ -126,18 +128,22 @@ class Oracle:
                                 "min_cut_gap": st[9]})
 
     def sv_anneal(self, inst: Instance, sa, sb, dt: float, mode: int = 0,
-                  want_state: bool = False) -> AnnealOut:
+                  want_state: bool = False, bias=None, sc=None) -> AnnealOut:
         h, ei, ej, ew, sa, sb = _d(inst.h), _i(inst.ei), _i(inst.ej), _d(inst.ew), _d(sa), _d(sb)
+        bias = None if bias is None else _d(bias)
+        sc = None if sc is None else _d(sc)
         n, steps = len(h), len(sa)
         s_arg = np.zeros(n, np.int8)
         s_sign = np.zeros(n, np.int8)
         ent = np.zeros(steps)
         st = np.zeros(5)
         state = np.zeros(2 << n) if want_state else None
-        self.lib.orc_sv_anneal(_ptr(h, _dp), n, _ptr(ei, _ip), _ptr(ej, _ip), _ptr(ew, _dp), len(ew),
-                               _ptr(sa, _dp), _ptr(sb, _dp), steps, dt, mode, _ptr(s_arg, _i8p),
-                               _ptr(s_sign, _i8p), _ptr(ent, _dp), _ptr(st, _dp),
-                               _ptr(state, _dp) if state is not None else None)
+        self.lib.orc_sv_anneal_bias(_ptr(h, _dp), n, _ptr(ei, _ip), _ptr(ej, _ip), _ptr(ew, _dp), len(ew),
+                                    _ptr(sa, _dp), _ptr(sb, _dp), steps, dt, mode, _ptr(s_arg, _i8p),
+                                    _ptr(s_sign, _i8p), _ptr(ent, _dp), _ptr(st, _dp),
+                                    _ptr(state, _dp) if state is not None else None,
+                                    _ptr(bias, _dp) if bias is not None else None,
+                                    _ptr(sc, _dp) if sc is not None else None)
         return AnnealOut(s_arg, st[0], st[1], st[2], 0.0, ent,
                          state=state.view(np.complex128) if state is not None else None,
                          extra={"sign_spins": s_sign, "sign_energy": st[3], "sign_prob": st[4]})

@@ -674,10 +674,26 @@ double orc_exact_ground(const double* h, int n, const int* ei, const int* ej, co
 // out_spins_argmax: quantum.rs readout; out_spins_sign: engine's sign<Z> readout.
 // out_state (optional): final amplitudes in the engine convention (bit i = physical
 // index, 0 <-> +1), normalised to the evolved norm.
+int orc_sv_anneal_bias(const double* h, int n, const int* ei, const int* ej, const double* ew, int m,
+                       const double* sa, const double* sb, int steps, double dt, int mode,
+                       int8_t* out_spins_argmax, int8_t* out_spins_sign, double* out_entropy,
+                       double* stats, double* out_state, const double* bias, const double* sc);
+
 int orc_sv_anneal(const double* h, int n, const int* ei, const int* ej, const double* ew, int m,
                   const double* sa, const double* sb, int steps, double dt, int mode,
                   int8_t* out_spins_argmax, int8_t* out_spins_sign, double* out_entropy,
                   double* stats, double* out_state) {
+    return orc_sv_anneal_bias(h, n, ei, ej, ew, m, sa, sb, steps, dt, mode, out_spins_argmax, out_spins_sign,
+                              out_entropy, stats, out_state, nullptr, nullptr);
+}
+
+// As orc_sv_anneal; in mode 1 an optional warm-start bias adds -C(s_k) sum_i b_i Z_i to the
+// single-site term (the engine's tessera_qa_problem.bias / schedule_c extension, not part
+// of the reference): g_i = -A X - (B h_i + C b_i) Z.
+int orc_sv_anneal_bias(const double* h, int n, const int* ei, const int* ej, const double* ew, int m,
+                       const double* sa, const double* sb, int steps, double dt, int mode,
+                       int8_t* out_spins_argmax, int8_t* out_spins_sign, double* out_entropy,
+                       double* stats, double* out_state, const double* bias, const double* sc) {
     const std::size_t dim = (std::size_t)1 << n;
     // Work in the engine basis: bit i = physical index s_i; spin = +1 when s_i = 0.
     std::vector<double> diag(dim);
@@ -727,7 +743,11 @@ int orc_sv_anneal(const double* h, int n, const int* ei, const int* ej, const do
             for (int i = 0; i < n; ++i) one_qubit(i, G);
             phase(B * dt * 0.5);
         } else {
-            for (int i = 0; i < n; ++i) { cplx G[2][2]; half_gate(A, B, h[i], dt, G); one_qubit(i, G); }
+            auto gate = [&](int i, cplx G[2][2]) {  // longitudinal field B h_i (+ C b_i)
+                if (bias) half_gate(A, 1.0, B * h[i] + sc[k] * bias[i], dt, G);
+                else half_gate(A, B, h[i], dt, G);
+            };
+            for (int i = 0; i < n; ++i) { cplx G[2][2]; gate(i, G); one_qubit(i, G); }
             // ZZ block: exp(-i dt * (-B sum_e w_e z_i z_j)), exact (diagonal, commuting).
             for (std::size_t x = 0; x < dim; ++x) {
                 double e = 0.0;
@@ -737,7 +757,7 @@ int orc_sv_anneal(const double* h, int n, const int* ei, const int* ej, const do
                 }
                 psi[x] *= std::exp(cplx(0, -dt * B * e));
             }
-            for (int i = 0; i < n; ++i) { cplx G[2][2]; half_gate(A, B, h[i], dt, G); one_qubit(i, G); }
+            for (int i = 0; i < n; ++i) { cplx G[2][2]; gate(i, G); one_qubit(i, G); }
         }
         if (out_entropy) out_entropy[k] = ent0();
     }

@@ -27,7 +27,7 @@ ST_JACOBI_NOT_CONVERGED, ST_BARRIER_TIMEOUT, ST_BAD_DIMS, ST_NONFINITE = 1, 2, 4
 class Problem(C.Structure):
     _fields_ = [("n", C.c_size_t), ("h", c_double_p), ("m", C.c_size_t), ("ei", c_size_p), ("ej", c_size_p),
                 ("ew", c_double_p), ("steps", C.c_size_t), ("schedule_a", c_double_p),
-                ("schedule_b", c_double_p)]
+                ("schedule_b", c_double_p), ("bias", c_double_p), ("schedule_c", c_double_p)]
 
 
 class Config(C.Structure):

@@ -85,6 +85,7 @@ struct ProblemHost {
     int n = 0, m = 0, steps = 0;
     std::vector<double> h, w, sa, sb;
     std::vector<int> ei, ej;
+    std::vector<double> bias, sc;  // empty = no warm-start bias
 };
 
 static ProblemHost validate_problem(const tessera_qa_problem* p) {
@@ -112,6 +113,15 @@ static ProblemHost validate_problem(const tessera_qa_problem* p) {
     P.sb.assign(p->schedule_b, p->schedule_b + p->steps);
     for (size_t k = 0; k < p->steps; ++k)
         if (!std::isfinite(P.sa[k]) || !std::isfinite(P.sb[k])) throw ArgError("schedule contains NaN/Inf");
+    if ((p->bias == nullptr) != (p->schedule_c == nullptr)) throw ArgError("bias and schedule_c go together");
+    if (p->bias) {
+        P.bias.assign(p->bias, p->bias + p->n);
+        P.sc.assign(p->schedule_c, p->schedule_c + p->steps);
+        for (double x : P.bias)
+            if (!std::isfinite(x)) throw ArgError("bias contains NaN/Inf");
+        for (double x : P.sc)
+            if (!std::isfinite(x)) throw ArgError("schedule_c contains NaN/Inf");
+    }
     return P;
 }
 
@@ -270,6 +280,8 @@ public:
         P_.w = P.w;
         P_.sa = P.sa;
         P_.sb = P.sb;
+        P_.bias = P.bias;
+        P_.sc = P.sc;
         upload_problem();
     }
 
@@ -492,6 +504,7 @@ private:
     int *dims_ = nullptr, *perm_ = nullptr, *counters_ = nullptr, *step_ = nullptr;
     double* scal_ = nullptr;
     double *sig2_ = nullptr, *sig_ = nullptr, *h_ = nullptr, *w_ = nullptr, *sa_ = nullptr, *sb_ = nullptr;
+    double *bias_ = nullptr, *sc_ = nullptr;
     double *entropy_ = nullptr, *dotout_ = nullptr, *amp2_ = nullptr;
     int8_t* spins_d_ = nullptr;
     GridBar* bar_ = nullptr;
@@ -514,7 +527,9 @@ private:
 
     size_t site_stride() const { return (size_t)2 * cap_ * cap_; }
     MpsView<T> mps() const { return MpsView<T>{sites_, dims_, n_, cap_, (long long)site_stride()}; }
-    ScheduleView schedule() const { return ScheduleView{h_, w_, sa_, sb_, step_, C_.dt, C_.dt / C_.ns}; }
+    ScheduleView schedule() const {
+        return ScheduleView{h_, w_, sa_, sb_, step_, C_.dt, C_.dt / C_.ns, bias_, sc_};
+    }
     SvdWork<T> work() const { return SvdWork<T>{theta_, W_, ld_, sig2_, sig_, perm_, counters_, scal_, bar_, stats_}; }
 
     double tol_for(int R) const {
@@ -589,6 +604,8 @@ private:
         add((void**)&w_, sizeof(double) * std::max(m_, 1));
         add((void**)&sa_, sizeof(double) * std::max(P_.steps, 1));
         add((void**)&sb_, sizeof(double) * std::max(P_.steps, 1));
+        add((void**)&bias_, sizeof(double) * n_);
+        add((void**)&sc_, sizeof(double) * std::max(P_.steps, 1));
         add((void**)&step_, sizeof(int));
         add((void**)&entropy_, sizeof(double) * std::max(P_.steps, 1));
         add((void**)&envs_, es * unit * 3);  // entropy chain: ONE, two ping-pong buffers
@@ -666,6 +683,14 @@ private:
         if (P_.steps) {
             TQ_CK(cudaMemcpyAsync(sa_, P_.sa.data(), sizeof(double) * P_.steps, cudaMemcpyHostToDevice, stream_));
             TQ_CK(cudaMemcpyAsync(sb_, P_.sb.data(), sizeof(double) * P_.steps, cudaMemcpyHostToDevice, stream_));
+        }
+        if (!P_.bias.empty()) {
+            TQ_CK(cudaMemcpyAsync(bias_, P_.bias.data(), sizeof(double) * n_, cudaMemcpyHostToDevice, stream_));
+            if (P_.steps)
+                TQ_CK(cudaMemcpyAsync(sc_, P_.sc.data(), sizeof(double) * P_.steps, cudaMemcpyHostToDevice, stream_));
+        } else {
+            TQ_CK(cudaMemsetAsync(bias_, 0, sizeof(double) * n_, stream_));
+            TQ_CK(cudaMemsetAsync(sc_, 0, sizeof(double) * std::max(P_.steps, 1), stream_));
         }
         TQ_CK(cudaStreamSynchronize(stream_));
     }

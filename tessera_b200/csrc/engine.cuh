@@ -44,6 +44,8 @@ struct ScheduleView {
     const int* step;    // device step counter (index into sa/sb)
     double dt;          // Trotter step
     double sub;         // dt / zz_substeps
+    const double* bias; // n warm-start bias b_i (zeros when unused)
+    const double* sc;   // steps, its weight C(s_k)
 };
 
 struct RunStats {

@@ -69,7 +69,8 @@ void launch_step_inc(int* step, cudaStream_t s) {
 }
 
 // ------------------------------------------------------------------------------------
-// K5: single-site half step.  g = -A X - B h Z = nx X + nz Z; exp(-i (dt/2) g) =
+// K5: single-site half step.  g = -A X - (B h + C b) Z = nx X + nz Z (C b: optional warm-start
+// bias field, zero when unused); exp(-i (dt/2) g) =
 // cos(phi) I - i sin(phi) (nx X + nz Z)/r with r = |(nx, nz)|, phi = r dt/2.
 // ------------------------------------------------------------------------------------
 template <typename T>
@@ -79,7 +80,7 @@ __device__ __forceinline__ void single_site_body(const MpsView<T>& mps, const Sc
     if (i >= mps.n) return;
     const int k = *sch.step;
     const double A = sch.sa[k], B = sch.sb[k];
-    const double nx = -A, nz = -B * sch.h[i];
+    const double nx = -A, nz = -(B * sch.h[i] + sch.sc[k] * sch.bias[i]);
     const double r = sqrt(nx * nx + nz * nz);
     double c = 1.0, sn = 0.0;
     if (r > 0) {

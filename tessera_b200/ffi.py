@@ -123,7 +123,7 @@ class AnnealResult:
     extra: dict = field(default_factory=dict)
 
 
-def problem_struct(h, ei, ej, ew, sa, sb):
+def problem_struct(h, ei, ej, ew, sa, sb, bias=None, sc=None):
     """Build a tessera_qa_problem; returns (struct, keepalive arrays)."""
     h = _arr(h, np.float64)
     ei = _arr(ei, np.uint64)
@@ -131,9 +131,13 @@ def problem_struct(h, ei, ej, ew, sa, sb):
     ew = _arr(ew, np.float64)
     sa = _arr(sa, np.float64)
     sb = _arr(sb, np.float64)
+    bias = None if bias is None else _arr(bias, np.float64)
+    sc = None if sc is None else _arr(sc, np.float64)
     P = _lib.Problem(len(h), _p(h, _lib.c_double_p), len(ew), _p(ei, _lib.c_size_p), _p(ej, _lib.c_size_p),
-                     _p(ew, _lib.c_double_p), len(sa), _p(sa, _lib.c_double_p), _p(sb, _lib.c_double_p))
-    return P, (h, ei, ej, ew, sa, sb)
+                     _p(ew, _lib.c_double_p), len(sa), _p(sa, _lib.c_double_p), _p(sb, _lib.c_double_p),
+                     _p(bias, _lib.c_double_p) if bias is not None else None,
+                     _p(sc, _lib.c_double_p) if sc is not None else None)
+    return P, (h, ei, ej, ew, sa, sb, bias, sc)
 
 
 def config_struct(dt=0.1, chi=32, precision="c128", zz_substeps=1, jacobi_tol=0.0, jacobi_max_sweeps=0,
@@ -163,14 +167,15 @@ def config_struct(dt=0.1, chi=32, precision="c128", zz_substeps=1, jacobi_tol=0.
 
 
 def anneal(h, ei, ej, ew, sa, sb, dt=0.1, chi=32, precision="c128", zz_substeps=1, want_checkpoint=False,
-           raise_on_status=True, checkpoint_out: np.ndarray | None = None, **kw) -> AnnealResult:
+           raise_on_status=True, checkpoint_out: np.ndarray | None = None, bias=None, sc=None,
+           **kw) -> AnnealResult:
     """tessera_qa_anneal_ex: the MPS-TEBD anneal with every result field.
 
     want_checkpoint returns the final MPS as checkpoint bytes; checkpoint_out (a contiguous uint8
     array of at least tessera_qa_checkpoint_bytes(n, chi) bytes, e.g. pinned memory) receives it
     in place instead."""
     L = _lib.load()
-    P, keep = problem_struct(h, ei, ej, ew, sa, sb)
+    P, keep = problem_struct(h, ei, ej, ew, sa, sb, bias, sc)
     c, keep2 = config_struct(dt=dt, chi=chi, precision=precision, zz_substeps=zz_substeps, **kw)
     n = int(P.n)
     k0 = int(c.step_begin)
@@ -366,7 +371,7 @@ def anneal_batch(problems, dt=None, chi=None, precision="c128", zz_substeps=1, w
     keep = []
     outs = []
     for b, p in enumerate(problems):
-        Pb, kp = problem_struct(p.h, p.ei, p.ej, p.ew, p.sa, p.sb)
+        Pb, kp = problem_struct(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, getattr(p, "bias", None), getattr(p, "sc", None))
         keep.append(kp)
         P_arr[b] = Pb
         cb, _ = config_struct(dt=dt if dt is not None else p.dt, chi=chi if chi is not None else p.chi,

@@ -25,6 +25,8 @@ class Problem:
     dt: float = 0.1
     chi: int = 32
     name: str = ""
+    bias: np.ndarray | None = None  # optional warm-start bias b_i (field -C(s) sum b_i Z_i)
+    sc: np.ndarray | None = None    # its schedule C(s_k)
 
     @property
     def n(self) -> int:
