@@ -165,6 +165,41 @@ TESSERA_QA_API int tessera_qa_svd(const double* a, size_t rows, size_t cols, dou
 TESSERA_QA_API int tessera_qa_svd_noalloc(const double* d_a, size_t rows, size_t cols, double* d_s, double* d_u,
                                           void* stream);
 
+/* Exact ground state by brute force over the 2^n patterns on the GPU (1 <= n <= 32): bit set
+ * <-> spin +1, first minimum kept, as rust/src/ising.rs:46-61 (exact_ground_state).  Writes n
+ * spins when out_spins is not NULL; returns the ground energy, or NaN on error. */
+TESSERA_QA_API double tessera_qa_exact_ground(const double* h, size_t n, const size_t* ei, const size_t* ej,
+                                              const double* ew, size_t m, int8_t* out_spins);
+
+/* ---- learned schedules: a message-passing GNN trained and run by the library's own kernels ----
+ * No counterpart in the reference's engine; python/gnn_guide.py:81-135 (its warm-start spin
+ * predictor) is the architectural starting point.  From an Ising graph it predicts `knots`
+ * monotone schedule knots 0 = s_0 <= ... <= s_{K-1} = 1 at equally spaced anneal times and a
+ * per-spin probability P(s_i = +1).  Weights are BF16 with FP32 accumulation (bf16_weights = 1)
+ * or FP32. */
+typedef struct tessera_qa_gnn tessera_qa_gnn;
+TESSERA_QA_API tessera_qa_gnn* tessera_qa_gnn_create(int hidden, int layers, int knots, uint64_t seed,
+                                                     int bf16_weights);
+TESSERA_QA_API void tessera_qa_gnn_destroy(tessera_qa_gnn* g);
+TESSERA_QA_API size_t tessera_qa_gnn_param_count(const tessera_qa_gnn* g);
+TESSERA_QA_API int tessera_qa_gnn_get_params(tessera_qa_gnn* g, float* out, size_t count);
+TESSERA_QA_API int tessera_qa_gnn_set_params(tessera_qa_gnn* g, const float* in, size_t count);
+/* out_knots: count x knots; out_p: total nodes (problems concatenated). */
+TESSERA_QA_API int tessera_qa_gnn_forward(tessera_qa_gnn* g, const tessera_qa_problem* problems, size_t count,
+                                          float* out_knots, float* out_p);
+/* One training step on a batch: loss = lambda_knots * mean (knot - target)^2 + lambda_spins *
+ * mean BCE(p_i, target_spins_i) over nodes whose target is 0 or 1 (negative = no label);
+ * forward and backward on the GPU, then Adam with step size lr (lr = 0: gradient only).
+ * out_grads (optional, param_count floats) receives the gradient. */
+TESSERA_QA_API int tessera_qa_gnn_train_step(tessera_qa_gnn* g, const tessera_qa_problem* problems, size_t count,
+                                             const float* target_knots, const float* target_spins, float lr,
+                                             float lambda_knots, float lambda_spins, float* out_loss,
+                                             float* out_grads, size_t grads_count);
+/* Schedule prediction (the learned layer's inference): out_knots count x knots; out_bias (total
+ * nodes, may be NULL) = 2 P(s_i = +1) - 1 in [-1, 1]. */
+TESSERA_QA_API int tessera_qa_schedule_predict(tessera_qa_gnn* g, const tessera_qa_problem* problems, size_t count,
+                                               double* out_knots, double* out_bias);
+
 /* Copies the calling thread's last error message into buf; returns its full length. */
 TESSERA_QA_API int tessera_qa_last_error(char* buf, size_t len);
 
