@@ -212,6 +212,7 @@ public:
         if (ev0_) cudaEventDestroy(ev0_);
         if (ev1_) cudaEventDestroy(ev1_);
         if (base_) cudaFree(base_);
+        if (res_base_) cudaFree(res_base_);
         if (obs_) cudaFree(obs_);
         if (stream_) cudaStreamDestroy(stream_);
     }
@@ -246,6 +247,23 @@ public:
         k_set_int<<<1, 1, 0, stream_>>>(step_, k0);
         TQ_CK(cudaGetLastError());
         TQ_CK(cudaEventRecord(ev0_, stream_));
+        // small bonds (theta fits one CTA's shared memory): the whole run is one launch of the
+        // resident anneal kernel, the same code a batch runs for each of its instances; the
+        // per-update path stays for large bonds, explicit Jacobi block widths and SVD timing
+        if (k1 > k0 && C_.block == 0 && !C_.timing && n_ >= 1) {
+            const int rc = std::max(8, (2 * cap_ + 7) & ~7);
+            ensure_resident(rc);
+            if (launch_anneal_resident<T>(res_inst_, res_ops_, res_off_, res_order_, 1, k0, k1, res_work_, rc,
+                                          stream_)) {
+                k_set_int<<<1, 1, 0, stream_>>>(step_, k1);
+                TQ_CK(cudaGetLastError());
+                launches_ += 2;
+                svd_launches_ += 1;
+                TQ_CK(cudaEventRecord(ev1_, stream_));
+                ran_ = true;
+                return;
+            }
+        }
         const ScheduleView sch = schedule();
         const MpsView<T> M = mps();
         for (int k = k0; k < k1; ++k) {
@@ -477,6 +495,7 @@ public:
         t.pp.tiny = sizeof(T) == 8 ? 1e-200 : 1e-60;
         t.pp.max_sweeps = C_.max_sweeps;
         t.pp.rows_cap = rows_cap;
+        t.pp.cols_cap = rows_cap;  // theta is at most 2 cap x 2 cap
         t.ent_steps = entc_;
         t.n_ent = n_ent_;
         t.pad = 0;
@@ -490,6 +509,27 @@ public:
     void mark_ran(double ms) { ran_ = false; last_ms_ = ms; }
     int max_sweeps_cfg() const { return C_.max_sweeps; }
     int* counters_ptr() const { return counters_; }
+    // device copies of this instance's task, gate list and work counter for the resident
+    // anneal kernel (made on first use)
+    void ensure_resident(int rows_cap) {
+        if (res_base_) return;
+        const size_t a1 = align256(sizeof(InstTask<T>));
+        const size_t a2 = a1 + align256(sizeof(GateOp) * std::max<size_t>(ops_.size(), 1));
+        TQ_CK(cudaMalloc(&res_base_, a2 + 256));
+        res_inst_ = reinterpret_cast<InstTask<T>*>(res_base_);
+        res_ops_ = reinterpret_cast<GateOp*>(res_base_ + a1);
+        res_off_ = reinterpret_cast<int*>(res_base_ + a2);
+        res_order_ = res_off_ + 2;
+        res_work_ = res_off_ + 4;
+        const InstTask<T> t = inst_task(step_, rows_cap);
+        const int hdr[4] = {0, (int)ops_.size(), 0, 0};
+        TQ_CK(cudaMemcpyAsync(res_inst_, &t, sizeof(t), cudaMemcpyHostToDevice, stream_));
+        if (!ops_.empty())
+            TQ_CK(cudaMemcpyAsync(res_ops_, ops_.data(), sizeof(GateOp) * ops_.size(), cudaMemcpyHostToDevice,
+                                  stream_));
+        TQ_CK(cudaMemcpyAsync(res_off_, hdr, sizeof(hdr), cudaMemcpyHostToDevice, stream_));
+        TQ_CK(cudaStreamSynchronize(stream_));
+    }
     double* scal_ptr() const { return scal_; }
     cudaStream_t own_stream() const { return stream_; }
 
@@ -500,6 +540,10 @@ private:
     cudaStream_t stream_ = nullptr;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     char* base_ = nullptr;
+    char* res_base_ = nullptr;
+    InstTask<T>* res_inst_ = nullptr;
+    GateOp* res_ops_ = nullptr;
+    int *res_off_ = nullptr, *res_order_ = nullptr, *res_work_ = nullptr;
     V *sites_ = nullptr, *theta_ = nullptr, *W_ = nullptr, *envs_ = nullptr, *xs_ = nullptr, *vbuf_ = nullptr;
     int *dims_ = nullptr, *perm_ = nullptr, *counters_ = nullptr, *step_ = nullptr;
     double* scal_ = nullptr;
@@ -797,15 +841,43 @@ public:
         }
         refs_off_[q_max_] = refs.size();
         nref_tot = refs.size();
-        const size_t bytes = 256 + sizeof(InstTask<T>) * B + sizeof(UpdRef) * std::max<size_t>(nref_tot, 1);
+        // per-instance gate lists for the resident whole-anneal kernel, and the order in which
+        // CTAs take instances: most work (gates x bond capacity^3) first
+        std::vector<GateOp> ops_all;
+        std::vector<int> op_off(B + 1, 0), order(B);
+        for (int b = 0; b < B; ++b) {
+            op_off[b] = (int)ops_all.size();
+            ops_all.insert(ops_all.end(), eng_[b]->ops().begin(), eng_[b]->ops().end());
+            order[b] = b;
+        }
+        op_off[B] = (int)ops_all.size();
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+            const double cx = (double)eng_[x]->ops().size() * std::pow((double)eng_[x]->cap(), 3.0);
+            const double cy = (double)eng_[y]->ops().size() * std::pow((double)eng_[y]->cap(), 3.0);
+            return cx > cy;
+        });
+        const size_t a0 = 256, a1 = a0 + align256(sizeof(InstTask<T>) * B);
+        const size_t a2 = a1 + align256(sizeof(UpdRef) * std::max<size_t>(nref_tot, 1));
+        const size_t a3 = a2 + align256(sizeof(GateOp) * std::max<size_t>(ops_all.size(), 1));
+        const size_t a4 = a3 + align256(sizeof(int) * (B + 1));
+        const size_t bytes = a4 + align256(sizeof(int) * B);
         TQ_CK(cudaMalloc(&base_, bytes));
         step_ = reinterpret_cast<int*>(base_);
-        insts_ = reinterpret_cast<InstTask<T>*>(base_ + 256);
-        refs_ = reinterpret_cast<UpdRef*>(base_ + 256 + sizeof(InstTask<T>) * B);
+        work_ = reinterpret_cast<int*>(base_ + 64);
+        insts_ = reinterpret_cast<InstTask<T>*>(base_ + a0);
+        refs_ = reinterpret_cast<UpdRef*>(base_ + a1);
+        ops_all_ = reinterpret_cast<GateOp*>(base_ + a2);
+        op_off_ = reinterpret_cast<int*>(base_ + a3);
+        order_ = reinterpret_cast<int*>(base_ + a4);
         std::vector<InstTask<T>> it;
         for (int b = 0; b < B; ++b) it.push_back(eng_[b]->inst_task(step_, rows_cap_));
         TQ_CK(cudaMemcpy(insts_, it.data(), sizeof(InstTask<T>) * B, cudaMemcpyHostToDevice));
         if (nref_tot) TQ_CK(cudaMemcpy(refs_, refs.data(), sizeof(UpdRef) * nref_tot, cudaMemcpyHostToDevice));
+        if (!ops_all.empty())
+            TQ_CK(cudaMemcpy(ops_all_, ops_all.data(), sizeof(GateOp) * ops_all.size(), cudaMemcpyHostToDevice));
+        TQ_CK(cudaMemcpy(op_off_, op_off.data(), sizeof(int) * (B + 1), cudaMemcpyHostToDevice));
+        TQ_CK(cudaMemcpy(order_, order.data(), sizeof(int) * B, cudaMemcpyHostToDevice));
+        resident_ = C[0].block == 0;
         for (auto& e : eng_) TQ_CK(cudaStreamSynchronize(e->own_stream()));
     }
     ~BatchEngine() override {
@@ -893,6 +965,18 @@ public:
         k_set_int<<<1, 1, 0, st_>>>(step_, k0);
         TQ_CK(cudaGetLastError());
         TQ_CK(cudaEventRecord(e0_, st_));
+        // small bonds: every step of every instance in one launch, one CTA per instance
+        if (resident_ && k1 > k0 &&
+            launch_anneal_resident<T>(insts_, ops_all_, op_off_, order_, B, k0, k1, work_, rows_cap_, st_)) {
+            k_set_int<<<1, 1, 0, st_>>>(step_, k1);
+            TQ_CK(cudaGetLastError());
+            launches_ += 2;
+            svd_launches_ += 1;
+            TQ_CK(cudaEventRecord(e1_, st_));
+            ran_ = true;
+            sync(nullptr);
+            return;
+        }
         for (int k = k0; k < k1; ++k) {
             launch_single_site_batch<T>(insts_, B, n_max_, cap_max_ * cap_max_, st_);
             for (int q = 0; q < q_max_; ++q) slot(q);
@@ -947,6 +1031,9 @@ private:
     int* step_ = nullptr;
     InstTask<T>* insts_ = nullptr;
     UpdRef* refs_ = nullptr;
+    GateOp* ops_all_ = nullptr;
+    int *op_off_ = nullptr, *order_ = nullptr, *work_ = nullptr;
+    bool resident_ = true;
     std::vector<size_t> refs_off_;
     int cap_max_ = 1, n_max_ = 1, q_max_ = 0, steps_ = 0, block_ = 8, rows_cap_ = 8;
     double ms_ = 0.0;

@@ -84,6 +84,7 @@ struct SvdParams {
     double tiny;       // columns with |w|^2 below this are never rotated
     int max_sweeps;
     int rows_cap;      // shared-memory column length
+    int cols_cap;      // shared-memory column count of the resident Jacobi (>= N, even)
 };
 
 struct ChainStep {
@@ -161,6 +162,11 @@ void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref,
                          cudaEvent_t svd_end = nullptr);
 template <typename T>
 void launch_entropy_batch(const InstTask<T>* insts, int ninst, cudaStream_t s);
+// Whole anneal of every instance, one CTA per instance at a time (small bonds only); false
+// when theta does not fit one CTA's shared memory.
+template <typename T>
+bool launch_anneal_resident(const InstTask<T>* insts, const GateOp* ops, const int* op_off, const int* order,
+                            int ninst, int k0, int k1, int* work, int rows_cap, cudaStream_t s);
 template <typename T>
 void launch_init_plus(const MpsView<T>& mps, cudaStream_t s);
 

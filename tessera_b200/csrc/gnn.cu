@@ -475,6 +475,8 @@ public:
         GN_CK(cudaMemcpy(host, w, sizeof(float) * Ly.total, cudaMemcpyDeviceToHost));
     }
     Wt weights() const { return Wt{w, bf16 ? wb : nullptr}; }
+    // the graph-head kernels index one thread per hidden unit and per knot
+    unsigned head_threads() const { return (unsigned)((std::max(64, std::max(Ly.H, Ly.K)) + 31) / 32 * 32); }
 
     void upload(const GnnBatchHost& B) {
         ensure(B.G, B.Nn, B.E);
@@ -504,7 +506,7 @@ public:
                                                               X(l + 1));
         }
         k_node_head<<<grid_of(Nn), 256, 0, st>>>(W, Ly.wn, Ly.bn, X(L), Nn, H, p);
-        k_graph_head<<<G, std::max(64, H), sizeof(float) * (2 * H + K), st>>>(W, Ly, X(L), d_goff, gmean, zpre, o,
+        k_graph_head<<<G, head_threads(), sizeof(float) * (2 * H + K), st>>>(W, Ly, X(L), d_goff, gmean, zpre, o,
                                                                               knots);
         GN_CK(cudaGetLastError());
     }
@@ -521,7 +523,7 @@ public:
         k_loss<<<1, 256, 0, st>>>(p, d_tn, Nn, knots, d_tk, G * K, ln, lk, inv_nlab, d_loss);
         GN_CK(cudaMemsetAsync(g, 0, sizeof(float) * Ly.total, st));
         GN_CK(cudaMemsetAsync(dx, 0, sizeof(float) * Nn * H, st));
-        k_graph_head_bwd<<<G, std::max(64, H), sizeof(float) * (2 * K + 2 * H), st>>>(W, Ly, G, gmean, zpre, o, knots,
+        k_graph_head_bwd<<<G, head_threads(), sizeof(float) * (2 * K + 2 * H), st>>>(W, Ly, G, gmean, zpre, o, knots,
                                                                                      d_tk, lk, d_goff, g, dx);
         k_node_head_bwd<<<grid_of((size_t)Nn * H), 256, 0, st>>>(W, Ly.wn, p, d_tn, Nn, H, ln, inv_nlab, dz, dx);
         k_wgrad_lin<<<grid_of(H + 1), 256, 0, st>>>(dz, Nn, 1, X(L), nullptr, H, nullptr, nullptr, 0, nullptr,

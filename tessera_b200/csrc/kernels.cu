@@ -284,6 +284,41 @@ __device__ __forceinline__ void group_reduce4(double v[4], double* red, int tid)
     }
 }
 
+// Rotation of a column pair from alpha = |w_p|^2 (v0), beta = |w_q|^2 (v1) and
+// gamma = w_p^H w_q (v2 + i v3), all accumulated in FP64.  Returns false for a converged
+// pair (|gamma|^2 <= tol^2 alpha beta, the FP64 convergence test) or a column below the
+// noise floor; else c, s and the phase e = gamma/|gamma| of
+//   w_p <- c w_p - s conj(e) w_q,   w_q <- s e w_p + c w_q,
+//   zeta = (beta - alpha) / (2|gamma|), t = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)),
+//   c = 1/sqrt(1 + t^2), s = c t.
+// 1/|gamma| comes from one FP64 rsqrt; in complex64 the tangent and cosine are formed in FP32
+// (the precision they are applied in).
+template <typename T>
+__device__ __forceinline__ bool jacobi_rotation(const double v0, const double v1, const double v2, const double v3,
+                                                const double tol, const double tiny, T& c, T& s, T& er, T& ei) {
+    const double g2 = v2 * v2 + v3 * v3;
+    if (!(v0 > tiny && v1 > tiny && g2 > tol * tol * (v0 * v1))) return false;
+    const double rg = rsqrt(g2);
+    const double zeta = 0.5 * (v1 - v0) * rg;
+    er = (T)(v2 * rg);
+    ei = (T)(v3 * rg);
+    if constexpr (sizeof(T) == 8) {
+        const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double cs = rsqrt(1.0 + t * t);
+        c = cs;
+        s = cs * t;
+    } else {
+        const float z = (float)zeta, az = fabsf(z);
+        // for |zeta| >= 1e18 1 + zeta^2 overflows float; t = 1/(2 zeta) to float precision there
+        const float ta = az < 1e18f ? 1.f / (az + sqrtf(1.f + az * az)) : 0.5f / az;
+        const float t = z >= 0.f ? ta : -ta;
+        const float cs = rsqrtf(1.f + t * t);
+        c = cs;
+        s = cs * t;
+    }
+    return true;
+}
+
 // Rotate local columns p, q (shared memory) of a group; returns 1 if rotated.
 template <typename T, int G>
 __device__ __forceinline__ int rotate_pair(cplx_t<T>* cp, cplx_t<T>* cq, bool valid, int R, double tol,
@@ -302,14 +337,8 @@ __device__ __forceinline__ int rotate_pair(cplx_t<T>* cp, cplx_t<T>* cq, bool va
     }
     group_reduce4<G>(v, red, tid);
     if (!valid) return 0;
-    const double al = v[0], be = v[1];
-    const double g = sqrt(v[2] * v[2] + v[3] * v[3]);
-    if (!(al > tiny && be > tiny && g > tol * sqrt(al * be))) return 0;
-    const double zeta = (be - al) / (2.0 * g);
-    const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-    const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
-    const T er = (T)(v[2] / g), ei = (T)(v[3] / g);
-    const T cc = (T)c, ss = (T)s;
+    T cc, ss, er, ei;
+    if (!jacobi_rotation<T>(v[0], v[1], v[2], v[3], tol, tiny, cc, ss, er, ei)) return 0;
     for (int r = lg; r < R; r += G) {
         const V x = cp[r], y = cq[r];
         // s conj(e) y and s e x
@@ -354,6 +383,99 @@ template <int BW, int RPL>
 struct SvdShape {
     static constexpr int NT = RPL > 0 ? 32 * BW : SVD_THREADS;
 };
+
+// ---- K3: sort + keep rule + discarded weight, by one CTA once wk.sig2 holds the column
+// norms.  Shared by the block-tournament and the resident Jacobi; `bytes` is the global
+// traffic the caller's Jacobi moved (run statistics).  red holds >= 4 (blockDim.x / 32) doubles.
+template <typename T>
+__device__ void svd_finish(const MpsView<T>& mps, const SvdWork<T>& wk, const SvdParams& pp, const int R, const int N,
+                           const double keep_floor, const int sweep, const bool converged, const double bytes,
+                           unsigned char* smraw, double* red) {
+    const int tid = threadIdx.x;
+    const int NT = blockDim.x, NW = NT >> 5;
+    int P2 = 1;
+    while (P2 < N) P2 <<= 1;
+    double* key = reinterpret_cast<double*>(smraw);  // [P2] then idx [P2]: 12 P2 bytes
+    int* idx = reinterpret_cast<int*>(key + P2);
+    for (int e = tid; e < P2; e += NT) {
+        key[e] = e < N ? wk.sig2[e] : -1.0;
+        idx[e] = e;
+    }
+    __syncthreads();
+    for (int k = 2; k <= P2; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int e = tid; e < P2; e += NT) {
+                const int o = e ^ j;
+                if (o > e) {
+                    const bool desc = ((e & k) == 0);
+                    const double ke = key[e], ko = key[o];
+                    const int ie = idx[e], io = idx[o];
+                    // "e before o" in descending order with ascending-index tie break
+                    const bool e_first = (ke > ko) || (ke == ko && ie < io);
+                    if (desc ? !e_first : e_first) {
+                        key[e] = ko; key[o] = ke; idx[e] = io; idx[o] = ie;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    const int kk = R < N ? R : N;
+    const int keep0 = pp.chi < kk ? pp.chi : kk;
+    double tot = 0.0, big = 0.0;
+    for (int e = tid; e < kk; e += NT) {
+        const double v = key[e] > 0 ? key[e] : 0.0;
+        tot += v;
+        if (e < keep0 && v >= keep_floor) big += 1.0;
+    }
+    tot = warp_sum(tot);
+    big = warp_sum(big);
+    if ((tid & 31) == 0) { red[(tid >> 5) * 4] = tot; red[(tid >> 5) * 4 + 1] = big; }
+    __syncthreads();
+    __shared__ int s_keep;
+    __shared__ double s_tot;
+    if (tid == 0) {
+        double t2 = 0.0, b2 = 0.0;
+        for (int w = 0; w < NW; ++w) { t2 += red[w * 4]; b2 += red[w * 4 + 1]; }
+        int keep = pp.no_trunc ? kk : (int)b2;
+        if (keep < 1) keep = 1;
+        s_keep = keep;
+        s_tot = t2;
+    }
+    __syncthreads();
+    const int keep = s_keep;
+    double disc = 0.0;
+    for (int e = keep + tid; e < kk; e += NT) disc += key[e] > 0 ? key[e] : 0.0;
+    disc = warp_sum(disc);
+    __syncthreads();
+    if ((tid & 31) == 0) red[(tid >> 5) * 4 + 2] = disc;
+    for (int e = tid; e < keep; e += NT) {
+        wk.perm[e] = idx[e];
+        wk.sig[e] = sqrt(key[e] > 0 ? key[e] : 0.0);
+    }
+    __syncthreads();
+    if (tid == 0 && !pp.no_trunc) {
+        double d2 = 0.0;
+        for (int w = 0; w < NW; ++w) d2 += red[w * 4 + 2];
+        RunStats* st = wk.stats;
+        if (s_tot > 0) {
+            const double ratio = d2 / s_tot;
+            if (ratio > st->max_trunc) st->max_trunc = ratio;
+        }
+        if (!isfinite(s_tot)) st->status |= ST_NONFINITE;
+        if (keep < kk && key[0] > 0) {
+            const double s0 = sqrt(key[0]), a = sqrt(fmax(key[keep - 1], 0.0)), b = sqrt(fmax(key[keep], 0.0));
+            const double deficit = 1.0 - (a - b) / s0;
+            if (deficit > st->gap_deficit) st->gap_deficit = deficit;
+        }
+        if (!converged) st->status |= ST_JACOBI_NOT_CONVERGED;
+        if (sweep > st->max_sweeps) st->max_sweeps = sweep;
+        st->svd_sweeps += sweep;
+        st->svd_bytes += bytes;
+        if (keep > st->max_bond) st->max_bond = keep;
+        st->updates += 1;
+        mps.dims[pp.bond + 1] = keep;
+    }
+}
 
 // Whole SVD of one theta by `ncta` cooperating CTAs (this one is number `cta`); with
 // ncta == 1 a single CTA runs every block pair itself and needs no grid barrier.
@@ -511,13 +633,8 @@ __device__ __forceinline__ void svd_body(const MpsView<T>& mps, const SvdWork<T>
                             v2 += __shfl_xor_sync(0xffffffffu, v2, o);
                             v3 += __shfl_xor_sync(0xffffffffu, v3, o);
                         }
-                        const double g = sqrt(v2 * v2 + v3 * v3);
-                        if (ok && v0 > tiny && v1 > tiny && g > pp.tol * sqrt(v0 * v1)) {
-                            const double zeta = (v1 - v0) / (2.0 * g);
-                            const double tt = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-                            const double cs = 1.0 / sqrt(1.0 + tt * tt);
-                            const T c = (T)cs, sn = (T)(cs * tt);
-                            const T er = (T)(v2 / g), ei = (T)(v3 / g);
+                        T c, sn, er, ei;
+                        if (ok && jacobi_rotation<T>(v0, v1, v2, v3, pp.tol, tiny, c, sn, er, ei)) {
 #pragma unroll
                             for (int k = 0; k < RPL; ++k) {
                                 const V x = xi[k], y = yj[k];
@@ -576,91 +693,452 @@ __device__ __forceinline__ void svd_body(const MpsView<T>& mps, const SvdWork<T>
     }
     if (!cta_sync(wk.bar, status, nblk)) return;
     if (cta != 0) return;
-    // ---- K3: sort + keep rule + discarded weight (CTA 0) ----
-    double* key = reinterpret_cast<double*>(smraw);
-    int* idx = reinterpret_cast<int*>(key + 4096);
-    int P2 = 1;
-    while (P2 < N) P2 <<= 1;
-    for (int e = tid; e < P2; e += NT) {
-        key[e] = e < N ? wk.sig2[e] : -1.0;
-        idx[e] = e;
+    svd_finish<T>(mps, wk, pp, R, N, keep_floor, sweep, converged,
+                  ((double)sweep * (P - 1) * 2.0 + 2.0) * (double)R * N * sizeof(V), smraw, red);
+}
+
+// ------------------------------------------------------------------------------------
+// K2r: resident one-sided Jacobi for small theta.  The whole R x N matrix stays in shared
+// memory (column c at col + c * rows_cap) for the entire SVD, so there is no staging and
+// no block structure: every round of the circle method over all N columns rotates N/2
+// disjoint pairs.  A pair is owned by LPP lanes (RPL complex rows per lane, R <= LPP RPL),
+// so a warp rotates 32/LPP pairs at once and the reduction is log2(LPP) shuffle levels;
+// alpha, beta, gamma are accumulated and reduced in FP64 and the rotation is
+// jacobi_rotation's.  A sweep is N-1 rounds; a sweep without a rotation ends the
+// iteration.  Rows per lane are capped at 8 and LPP grows with R: (LPP, RPL) = (8, R/8)
+// up to R = 64, then (16, 8) and (32, 8).
+// ------------------------------------------------------------------------------------
+constexpr int RES_MAXT = 512;
+
+template <typename T, int LPP, int RPL>
+__device__ void jacobi_core(cplx_t<T>* col, const int rc, const int R, const int N, const double tol,
+                            const double tiny, const int max_sweeps, int* s_rot, int& sweeps, bool& converged) {
+    using V = cplx_t<T>;
+    constexpr int PPW = 32 / LPP;
+    const int tid = threadIdx.x, NW = blockDim.x >> 5, warp = tid >> 5, lane = tid & 31;
+    const int sub = lane / LPP, sl = lane % LPP;
+    const int Nc = N + (N & 1);
+    const int npairs = Nc / 2;
+    if (tid == 0) {
+        s_rot[0] = 0;
+        s_rot[1] = 0;
     }
     __syncthreads();
-    for (int k = 2; k <= P2; k <<= 1)
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int e = tid; e < P2; e += NT) {
-                const int o = e ^ j;
-                if (o > e) {
-                    const bool desc = ((e & k) == 0);
-                    const double ke = key[e], ko = key[o];
-                    const int ie = idx[e], io = idx[o];
-                    // "e before o" in descending order with ascending-index tie break
-                    const bool e_first = (ke > ko) || (ke == ko && ie < io);
-                    if (desc ? !e_first : e_first) {
-                        key[e] = ko; key[o] = ke; idx[e] = io; idx[o] = ie;
+    int sweep = 0;
+    converged = false;
+    for (; sweep < max_sweeps; ++sweep) {
+        int rot = 0;
+        for (int r = 0; r < Nc - 1; ++r) {
+            for (int base = warp * PPW; base < npairs; base += NW * PPW) {  // warp-uniform
+                const int pr = base + sub;
+                int p = N, q = N;
+                if (pr < npairs) tournament(Nc, r, pr, p, q);
+                const bool ok = p < N && q < N;
+                V* cp = col + (ok ? p : 0) * rc;
+                V* cq = col + (ok ? q : 0) * rc;
+                V x[RPL], y[RPL];
+#pragma unroll
+                for (int k = 0; k < RPL; ++k) {
+                    const int row = sl + LPP * k;
+                    const bool in = ok && row < R;
+                    x[k] = in ? cp[row] : czero<V>();
+                    y[k] = in ? cq[row] : czero<V>();
+                }
+                double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+#pragma unroll
+                for (int k = 0; k < RPL; ++k) {
+                    v0 += (double)x[k].x * x[k].x + (double)x[k].y * x[k].y;
+                    v1 += (double)y[k].x * y[k].x + (double)y[k].y * y[k].y;
+                    v2 += (double)x[k].x * y[k].x + (double)x[k].y * y[k].y;
+                    v3 += (double)x[k].x * y[k].y - (double)x[k].y * y[k].x;
+                }
+#pragma unroll
+                for (int o = LPP / 2; o > 0; o >>= 1) {
+                    v0 += __shfl_xor_sync(0xffffffffu, v0, o);
+                    v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+                    v2 += __shfl_xor_sync(0xffffffffu, v2, o);
+                    v3 += __shfl_xor_sync(0xffffffffu, v3, o);
+                }
+                T c, sn, er, ei;
+                if (ok && jacobi_rotation<T>(v0, v1, v2, v3, tol, tiny, c, sn, er, ei)) {
+#pragma unroll
+                    for (int k = 0; k < RPL; ++k) {
+                        const int row = sl + LPP * k;
+                        const V xv = x[k], yv = y[k];
+                        const T ey_re = er * yv.x + ei * yv.y, ey_im = er * yv.y - ei * yv.x;
+                        const T ex_re = er * xv.x - ei * xv.y, ex_im = er * xv.y + ei * xv.x;
+                        if (row < R) {
+                            cp[row] = mk<V>(c * xv.x - sn * ey_re, c * xv.y - sn * ey_im);
+                            cq[row] = mk<V>(sn * ex_re + c * yv.x, sn * ex_im + c * yv.y);
+                        }
                     }
+                    if (sl == 0) ++rot;
                 }
             }
             __syncthreads();
         }
-    const int kk = R < N ? R : N;
-    const int keep0 = pp.chi < kk ? pp.chi : kk;
-    double tot = 0.0, big = 0.0;
-    for (int e = tid; e < kk; e += NT) {
-        const double v = key[e] > 0 ? key[e] : 0.0;
-        tot += v;
-        if (e < keep0 && v >= keep_floor) big += 1.0;
+        // per-sweep rotation count in alternating slots: the slot read here is reset only
+        // after the barrier that ends the next sweep's first round
+        if (rot) atomicAdd(&s_rot[sweep & 1], rot);
+        __syncthreads();
+        const int done = s_rot[sweep & 1];
+        if (tid == 0) s_rot[(sweep + 1) & 1] = 0;
+        if (done == 0) {
+            converged = true;
+            ++sweep;
+            break;
+        }
     }
-    tot = warp_sum(tot);
-    big = warp_sum(big);
-    if ((tid & 31) == 0) { red[(tid >> 5) * 4] = tot; red[(tid >> 5) * 4 + 1] = big; }
+    sweeps = sweep;
     __syncthreads();
-    __shared__ int s_keep;
-    __shared__ double s_tot;
+}
+
+// sum of |w|^2 over an R x N shared-memory matrix, returned to every thread
+template <typename T>
+__device__ double block_fro2(const cplx_t<T>* col, const int rc, const int R, const int N, double* red) {
+    using V = cplx_t<T>;
+    __shared__ double s_sum;
+    const int tid = threadIdx.x, NW = blockDim.x >> 5, warp = tid >> 5, lane = tid & 31;
+    double part = 0.0;
+    for (int c = warp; c < N; c += NW) {
+        const V* w = col + c * rc;
+        double sj = 0.0;
+        for (int r = lane; r < R; r += 32) sj += (double)w[r].x * w[r].x + (double)w[r].y * w[r].y;
+        part += warp_sum(sj);
+    }
+    if (lane == 0) red[warp] = part;
+    __syncthreads();
     if (tid == 0) {
-        double t2 = 0.0, b2 = 0.0;
-        for (int w = 0; w < NW; ++w) { t2 += red[w * 4]; b2 += red[w * 4 + 1]; }
-        int keep = pp.no_trunc ? kk : (int)b2;
-        if (keep < 1) keep = 1;
-        s_keep = keep;
-        s_tot = t2;
+        double b = 0.0;
+        for (int w = 0; w < NW; ++w) b += red[w];
+        s_sum = b;
     }
     __syncthreads();
-    const int keep = s_keep;
-    double disc = 0.0;
-    for (int e = keep + tid; e < kk; e += NT) disc += key[e] > 0 ? key[e] : 0.0;
-    disc = warp_sum(disc);
-    __syncthreads();
-    if ((tid & 31) == 0) red[(tid >> 5) * 4 + 2] = disc;
-    for (int e = tid; e < keep; e += NT) {
-        wk.perm[e] = idx[e];
-        wk.sig[e] = sqrt(key[e] > 0 ? key[e] : 0.0);
-    }
-    __syncthreads();
-    if (tid == 0 && !pp.no_trunc) {
-        double d2 = 0.0;
-        for (int w = 0; w < NW; ++w) d2 += red[w * 4 + 2];
-        RunStats* st = wk.stats;
-        if (s_tot > 0) {
-            const double ratio = d2 / s_tot;
-            if (ratio > st->max_trunc) st->max_trunc = ratio;
+    return s_sum;
+}
+
+// column norms of the shared-memory matrix into wk.sig2 (optionally writing the columns to W)
+template <typename T>
+__device__ void resident_norms(const cplx_t<T>* col, const int rc, const int R, const int N, cplx_t<T>* W,
+                               const int ld, double* sig2) {
+    using V = cplx_t<T>;
+    const int NW = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int c = warp; c < N; c += NW) {
+        const V* src = col + c * rc;
+        double sj = 0.0;
+        for (int r = lane; r < R; r += 32) {
+            const V w = src[r];
+            if (W) W[(long long)c * ld + r] = w;
+            sj += (double)w.x * w.x + (double)w.y * w.y;
         }
-        if (!isfinite(s_tot)) st->status |= ST_NONFINITE;
-        if (keep < kk && key[0] > 0) {
-            const double s0 = sqrt(key[0]), a = sqrt(fmax(key[keep - 1], 0.0)), b = sqrt(fmax(key[keep], 0.0));
-            const double deficit = 1.0 - (a - b) / s0;
-            if (deficit > st->gap_deficit) st->gap_deficit = deficit;
-        }
-        if (!converged) st->status |= ST_JACOBI_NOT_CONVERGED;
-        if (sweep > st->max_sweeps) st->max_sweeps = sweep;
-        st->svd_sweeps += sweep;
-        // staged reads + write-backs of every block pair in every round, plus the norm pre-pass
-        // and the final column norms
-        st->svd_bytes += ((double)sweep * (P - 1) * 2.0 + 2.0) * (double)R * N * sizeof(V);
-        if (keep > st->max_bond) st->max_bond = keep;
-        st->updates += 1;
-        mps.dims[pp.bond + 1] = keep;
+        sj = warp_sum(sj);
+        if (lane == 0) sig2[c] = sj;
     }
+    __syncthreads();
+}
+
+__device__ __forceinline__ double noise_tiny(double pp_tiny, int R, double fro2, bool single) {
+    const double ulp = single ? 1.1920928955078125e-07 : 2.220446049250313e-16;
+    const double floor_rel = 8.0 * sqrt((double)R) * ulp;
+    return fmax(pp_tiny, floor_rel * floor_rel * fro2);
+}
+
+template <typename T, int LPP, int RPL>
+__device__ void svd_resident_body(const MpsView<T>& mps, const SvdWork<T>& wk, const SvdParams& pp,
+                                  unsigned char* smraw) {
+    using V = cplx_t<T>;
+    const int NW = blockDim.x >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    __shared__ double red[4 * 32];
+    __shared__ int s_rot[2];
+    const int R = pp.R > 0 ? pp.R : 2 * mps.dims[pp.bond];
+    const int N = pp.N > 0 ? pp.N : 2 * mps.dims[pp.bond + 2];
+    const int rc = pp.rows_cap;
+    V* col = reinterpret_cast<V*>(smraw);  // [cols_cap][rows_cap]
+    if (R > rc || R > LPP * RPL || N > pp.cols_cap) {  // host sizing bug guard
+        if (tid == 0) atomicOr(&wk.stats->status, ST_BAD_DIMS);
+        return;
+    }
+    const int ld = wk.ld;
+    for (int c = warp; c < N; c += NW) {
+        const V* src = wk.W + (long long)c * ld;
+        V* dst = col + c * rc;
+        for (int r = lane; r < R; r += 32) dst[r] = src[r];
+    }
+    __syncthreads();
+    const double tiny = noise_tiny(pp.tiny, R, block_fro2<T>(col, rc, R, N, red), sizeof(T) == 4);
+    int sweep = 0;
+    bool converged = false;
+    jacobi_core<T, LPP, RPL>(col, rc, R, N, pp.tol, tiny, pp.max_sweeps, s_rot, sweep, converged);
+    resident_norms<T>(col, rc, R, N, wk.W, ld, wk.sig2);
+    svd_finish<T>(mps, wk, pp, R, N, fmax(1e-28, tiny), sweep, converged, 2.0 * (double)R * N * sizeof(V), smraw,
+                  red);
+}
+
+template <typename T, int LPP, int RPL>
+__global__ void __launch_bounds__(RES_MAXT, 1) k_svd_res(MpsView<T> mps, SvdWork<T> wk, SvdParams pp) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    svd_resident_body<T, LPP, RPL>(mps, wk, pp, smraw);
+}
+
+template <typename T, int LPP, int RPL>
+__global__ void __launch_bounds__(RES_MAXT, 1) k_svd_res_batch(const InstTask<T>* insts, const UpdRef* refs,
+                                                              int nref) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    for (int t = blockIdx.x; t < nref; t += gridDim.x) {
+        const UpdRef rf = refs[t];
+        const InstTask<T>& it = insts[rf.inst];
+        SvdParams pp = it.pp;
+        pp.bond = rf.op.bond;
+        svd_resident_body<T, LPP, RPL>(it.mps, it.wk, pp, smraw);
+        __syncthreads();
+    }
+}
+
+template <typename T>
+__device__ void chain_body(const MpsView<T>& mps, int right, const ChainStep* steps, int nsteps, cplx_t<T>* envs,
+                           cplx_t<T>* X, GridBar* bar, RunStats* stats, int cta, int ncta);
+template <typename T>
+__device__ void entropy_body(const MpsView<T>& mps, const cplx_t<T>* r1, double* out, const int* step);
+
+// ------------------------------------------------------------------------------------
+// K8: the whole anneal of small-bond instances, one CTA per instance at a time.  A CTA
+// takes the next instance (longest first) from a work counter and runs every Trotter step
+// of it: single-site half step, every two-site update of the ZZ block in order (theta
+// quads formed straight into shared memory, resident Jacobi, keep rule, absorption from
+// shared memory), single-site half step, qubit-0 entropy.  Nothing waits on another CTA,
+// so instances never wait for the slowest SVD of a gate slot and the whole run is one
+// launch.  256 threads (the environment GEMMs of the entropy step use 256).
+// ------------------------------------------------------------------------------------
+template <typename T, int LPP, int RPL>
+__device__ void resident_update(const MpsView<T>& mps, const ScheduleView& sch, const GateOp& op,
+                                const SvdWork<T>& wk, const SvdParams& pp0, cplx_t<T>* col, unsigned char* sortbuf,
+                                double* red, int* s_rot) {
+    using V = cplx_t<T>;
+    const int tid = threadIdx.x, NT = blockDim.x;
+    const int i = op.bond;
+    const int dl = mps.dims[i], mid = mps.dims[i + 1], dr = mps.dims[i + 2];
+    const int R = 2 * dl, N = 2 * dr, rc = pp0.rows_cap, ld = wk.ld, cap = mps.cap;
+    if (R > rc || R > LPP * RPL || N > pp0.cols_cap) {
+        if (tid == 0) atomicOr(&wk.stats->status, ST_BAD_DIMS);
+        return;
+    }
+    // theta[(2a + r1), (r2 dr + b)] = sum_{s1 s2} G[r1 r2][s1 s2] sum_c A[(2a+s1), c] C[(2c+s2), b]
+    {
+        V g[16];
+        gate_of(op, sch, nullptr, g);
+        const V* A = mps.site(i);
+        const V* Cm = mps.site(i + 1);
+        for (int e = tid; e < dl * dr; e += NT) {
+            const int a = e / dr, b = e - a * dr;
+            V acc[2][2];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) (&acc[0][0])[q] = czero<V>();
+            const V* a0 = A + (long long)(2 * a) * cap;
+            const V* a1 = a0 + cap;
+            for (int c = 0; c < mid; ++c) {
+                const V x0 = a0[c], x1 = a1[c];
+                const V y0 = Cm[(long long)(2 * c) * cap + b], y1 = Cm[(long long)(2 * c + 1) * cap + b];
+                cfma(acc[0][0], x0, y0); cfma(acc[0][1], x0, y1);
+                cfma(acc[1][0], x1, y0); cfma(acc[1][1], x1, y1);
+            }
+#pragma unroll
+            for (int r1 = 0; r1 < 2; ++r1)
+#pragma unroll
+                for (int r2 = 0; r2 < 2; ++r2) {
+                    V o = czero<V>();
+#pragma unroll
+                    for (int s1 = 0; s1 < 2; ++s1)
+#pragma unroll
+                        for (int s2 = 0; s2 < 2; ++s2) cfma(o, g[(r1 * 2 + r2) * 4 + s1 * 2 + s2], acc[s1][s2]);
+                    const int row = 2 * a + r1, cc = r2 * dr + b;
+                    col[cc * rc + row] = o;
+                    wk.theta[(long long)cc * ld + row] = o;
+                }
+        }
+    }
+    __syncthreads();
+    const double tiny = noise_tiny(pp0.tiny, R, block_fro2<T>(col, rc, R, N, red), sizeof(T) == 4);
+    int sweep = 0;
+    bool converged = false;
+    jacobi_core<T, LPP, RPL>(col, rc, R, N, pp0.tol, tiny, pp0.max_sweeps, s_rot, sweep, converged);
+    resident_norms<T>(col, rc, R, N, nullptr, ld, wk.sig2);
+    SvdParams pp = pp0;
+    pp.bond = i;
+    // global traffic of the update: A and C read, theta written and read back, A' and C' written
+    const double bytes = (double)sizeof(V) * (2.0 * dl * mid + 2.0 * mid * dr + 3.0 * R * N);
+    svd_finish<T>(mps, wk, pp, R, N, fmax(1e-28, tiny), sweep, converged, bytes, sortbuf, red);
+    __syncthreads();
+    const int keep = mps.dims[i + 1];
+    // A' (a, s1, k) = W[(2a+s1), perm k] / sigma_k
+    V* An = mps.site(i);
+    for (int e = tid; e < R * keep; e += NT) {
+        const int row = e / keep, k = e - row * keep;
+        const double inv = 1.0 / wk.sig[k];
+        const V w = col[wk.perm[k] * rc + row];
+        An[(long long)row * cap + k] = mk<V>((T)(w.x * inv), (T)(w.y * inv));
+    }
+    // C' (k, s2, b) = (1/sigma_k) sum_row conj(W[row, perm k]) theta[row, s2 dr + b]
+    V* Cn = mps.site(i + 1);
+    for (int e = tid; e < keep * N; e += NT) {
+        const int k = e / N, j = e - k * N;
+        const V* u = col + wk.perm[k] * rc;
+        const V* t = wk.theta + (long long)j * ld;
+        double re = 0.0, im = 0.0;
+        for (int row = 0; row < R; ++row) {
+            const V uu = u[row], tt = t[row];
+            re += (double)uu.x * tt.x + (double)uu.y * tt.y;
+            im += (double)uu.x * tt.y - (double)uu.y * tt.x;
+        }
+        const double inv = 1.0 / wk.sig[k];
+        const int s2 = j >= dr ? 1 : 0, b = j - s2 * dr;
+        Cn[(long long)(2 * k + s2) * cap + b] = mk<V>((T)(re * inv), (T)(im * inv));
+    }
+    __syncthreads();
+}
+
+template <typename T, int LPP, int RPL>
+__global__ void __launch_bounds__(256) k_anneal_res(const InstTask<T>* insts, const GateOp* ops, const int* op_off,
+                                                    const int* order, int ninst, int k0, int k1, int* work,
+                                                    size_t col_bytes) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ double red[4 * 32];
+    __shared__ int s_rot[2];
+    __shared__ int s_step;
+    __shared__ int s_idx;
+    const int tid = threadIdx.x;
+    cplx_t<T>* col = reinterpret_cast<cplx_t<T>*>(smraw);
+    unsigned char* sortbuf = smraw + col_bytes;
+    for (;;) {
+        if (tid == 0) s_idx = atomicAdd(work, 1);
+        __syncthreads();
+        const int idx = s_idx;
+        __syncthreads();
+        if (idx >= ninst) break;
+        const int b = order[idx];
+        const InstTask<T>& it = insts[b];
+        const MpsView<T> mps = it.mps;
+        ScheduleView sch = it.sch;
+        sch.step = &s_step;
+        const int q0 = op_off[b], q1 = op_off[b + 1];
+        for (int k = k0; k < k1; ++k) {
+            if (tid == 0) s_step = k;
+            __syncthreads();
+            for (int i = 0; i < mps.n; ++i) single_site_body<T>(mps, sch, i, 0, 1);
+            __syncthreads();
+            for (int q = q0; q < q1; ++q)
+                resident_update<T, LPP, RPL>(mps, sch, ops[q], it.wk, it.pp, col, sortbuf, red, s_rot);
+            for (int i = 0; i < mps.n; ++i) single_site_body<T>(mps, sch, i, 0, 1);
+            __syncthreads();
+            if (mps.n >= 2) {
+                chain_body<T>(mps, 1, it.ent_steps, it.n_ent, it.envs, it.X, nullptr, it.wk.stats, 0, 1);
+                __syncthreads();
+                entropy_body<T>(mps, it.envs + it.r1_off, it.entropy, &s_step);
+            } else {
+                entropy_body<T>(mps, nullptr, it.entropy, &s_step);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Shared memory of the resident kernels for a rows_cap x cols_cap theta (0: does not fit).
+// with_cols: the sort buffer follows the matrix instead of overlaying it.
+template <typename T>
+static size_t resident_smem(int rows_cap, int cols_cap, bool with_cols = false) {
+    int P2 = 1;
+    while (P2 < cols_cap) P2 <<= 1;
+    const size_t m = sizeof(cplx_t<T>) * (size_t)rows_cap * cols_cap;
+    const size_t sort = (size_t)P2 * (sizeof(double) + sizeof(int));
+    const size_t b = with_cols ? ((m + 15) & ~(size_t)15) + sort : (m < sort ? sort : m);
+    return (rows_cap <= 256 && b <= 200 * 1024) ? b : 0;
+}
+
+// (LPP, RPL) for a row count: the index of the smallest shape with LPP RPL >= rows_cap
+static int resident_shape(int rows_cap) {
+    if (rows_cap <= 8) return 0;
+    if (rows_cap <= 16) return 1;
+    if (rows_cap <= 32) return 2;
+    if (rows_cap <= 64) return 3;
+    if (rows_cap <= 128) return 4;
+    if (rows_cap <= 256) return 5;
+    return -1;
+}
+
+#define TQ_RES_SHAPES(F)             \
+    switch (resident_shape(pp.rows_cap)) { \
+        case 0: F(8, 1); break;       \
+        case 1: F(8, 2); break;       \
+        case 2: F(8, 4); break;       \
+        case 3: F(8, 8); break;       \
+        case 4: F(16, 8); break;      \
+        case 5: F(32, 8); break;      \
+        default: return false;        \
+    }
+
+// Launch one resident-Jacobi kernel (single theta when insts == nullptr, else a batch).
+template <typename T, int LPP, int RPL>
+static void res_launch(const MpsView<T>* mps, const SvdWork<T>* wk, const SvdParams& pp, const InstTask<T>* insts,
+                       const UpdRef* refs, int nref, cudaStream_t s) {
+    const size_t smem = resident_smem<T>(pp.rows_cap, pp.cols_cap);
+    const int pairs = pp.cols_cap / 2;
+    const int warps = (pairs + (32 / LPP) - 1) / (32 / LPP);
+    int nt = 32 * (warps < 1 ? 1 : warps);
+    if (nt > RES_MAXT) nt = RES_MAXT;
+    if (insts) {
+        auto fn = k_svd_res_batch<T, LPP, RPL>;
+        TQ_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        TQ_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, nt, smem));
+        if (per_sm < 1) throw std::runtime_error("k_svd_res_batch does not fit on an SM");
+        int grid = per_sm * num_sms();
+        if (grid > nref) grid = nref;
+        fn<<<grid, nt, smem, s>>>(insts, refs, nref);
+    } else {
+        auto fn = k_svd_res<T, LPP, RPL>;
+        TQ_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        fn<<<1, nt, smem, s>>>(*mps, *wk, pp);
+    }
+    TQ_CHECK(cudaGetLastError());
+}
+
+template <typename T>
+static bool res_dispatch(const MpsView<T>* mps, const SvdWork<T>* wk, const SvdParams& pp, const InstTask<T>* insts,
+                         const UpdRef* refs, int nref, cudaStream_t s) {
+    if (!resident_smem<T>(pp.rows_cap, pp.cols_cap)) return false;
+#define TQ_F(L, RP) res_launch<T, L, RP>(mps, wk, pp, insts, refs, nref, s)
+    TQ_RES_SHAPES(TQ_F)
+#undef TQ_F
+    return true;
+}
+
+template <typename T, int LPP, int RPL>
+static void anneal_res_launch(const InstTask<T>* insts, const GateOp* ops, const int* op_off, const int* order,
+                              int ninst, int k0, int k1, int* work, int rows_cap, cudaStream_t s) {
+    const size_t smem = resident_smem<T>(rows_cap, rows_cap, true);
+    const size_t col_bytes = (sizeof(cplx_t<T>) * (size_t)rows_cap * rows_cap + 15) & ~(size_t)15;
+    auto fn = k_anneal_res<T, LPP, RPL>;
+    TQ_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    TQ_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, smem));
+    if (per_sm < 1) throw std::runtime_error("k_anneal_res does not fit on an SM");
+    int grid = per_sm * num_sms();
+    if (grid > ninst) grid = ninst;
+    TQ_CHECK(cudaMemsetAsync(work, 0, sizeof(int), s));
+    fn<<<grid, 256, smem, s>>>(insts, ops, op_off, order, ninst, k0, k1, work, col_bytes);
+    TQ_CHECK(cudaGetLastError());
+}
+
+template <typename T>
+bool launch_anneal_resident(const InstTask<T>* insts, const GateOp* ops, const int* op_off, const int* order,
+                            int ninst, int k0, int k1, int* work, int rows_cap, cudaStream_t s) {
+    if (!resident_smem<T>(rows_cap, rows_cap, true)) return false;
+    SvdParams pp{};
+    pp.rows_cap = rows_cap;
+#define TQ_F(L, RP) anneal_res_launch<T, L, RP>(insts, ops, op_off, order, ninst, k0, k1, work, rows_cap, s)
+    TQ_RES_SHAPES(TQ_F)
+#undef TQ_F
+    return true;
 }
 
 template <typename T, int BW, int RPL>
@@ -723,6 +1201,10 @@ int launch_svd(const MpsView<T>& mps, int bond, int chi, double tol, int max_swe
     pp.max_sweeps = max_sweeps;
     pp.rows_cap = (rows_ub + 7) & ~7;
     if (pp.rows_cap < 8) pp.rows_cap = 8;
+    pp.cols_cap = (cols_ub + 1) & ~1;
+    if (pp.cols_cap < 2) pp.cols_cap = 2;
+    // small theta: the whole matrix stays in one CTA's shared memory
+    if (res_dispatch<T>(&mps, &wk, pp, nullptr, nullptr, 0, s)) return 1;
     TQ_CHECK(cudaMemsetAsync(wk.counters, 0, sizeof(int) * max_sweeps, s));
     TQ_CHECK(cudaMemsetAsync(wk.scal, 0, sizeof(double) * 2, s));
     // register-resident path for rows <= 512: rows per lane = next power of two >= rows/32
@@ -1163,13 +1645,18 @@ void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref,
     int bw = block_w < 4 ? 4 : block_w;
     if (rpl == 16 && bw > 8) bw = 8;
     if (svd_begin) TQ_CHECK(cudaEventRecord(svd_begin, s));
+    SvdParams rp{};
+    rp.rows_cap = rows_cap;
+    rp.cols_cap = rows_cap;  // every instance's theta is at most rows_ub x rows_ub
+    if (!res_dispatch<T>(nullptr, nullptr, rp, insts, refs, nref, s)) {
 #define TQ_RB(B, RP) \
     if (bw == B && rpl == RP) { svd_batch_bw<T, B, RP>(insts, refs, nref, rows_cap, s); } else
-    TQ_RB(4, 1) TQ_RB(4, 2) TQ_RB(4, 4) TQ_RB(4, 8) TQ_RB(4, 16)
-    TQ_RB(8, 1) TQ_RB(8, 2) TQ_RB(8, 4) TQ_RB(8, 8) TQ_RB(8, 16)
-    TQ_RB(16, 1) TQ_RB(16, 2) TQ_RB(16, 4) TQ_RB(16, 8)
-    throw std::runtime_error("unsupported Jacobi block width");
+        TQ_RB(4, 1) TQ_RB(4, 2) TQ_RB(4, 4) TQ_RB(4, 8) TQ_RB(4, 16)
+        TQ_RB(8, 1) TQ_RB(8, 2) TQ_RB(8, 4) TQ_RB(8, 8) TQ_RB(8, 16)
+        TQ_RB(16, 1) TQ_RB(16, 2) TQ_RB(16, 4) TQ_RB(16, 8)
+        throw std::runtime_error("unsupported Jacobi block width");
 #undef TQ_RB
+    }
     if (svd_end) TQ_CHECK(cudaEventRecord(svd_end, s));
     const int keep_tiles = (d_ub + 31) / 32;
     k_absorb_u_batch<T><<<dim3(keep_tiles, (2 * d_ub + 7) / 8, nref), dim3(32, 8), 0, s>>>(insts, refs);
@@ -1218,7 +1705,9 @@ void launch_entropy_batch(const InstTask<T>* insts, int ninst, cudaStream_t s) {
     template void launch_single_site_batch<T>(const InstTask<T>*, int, int, int, cudaStream_t);                \
     template void launch_update_batch<T>(const InstTask<T>*, const UpdRef*, int, int, int, int, cudaStream_t,  \
                                          cudaEvent_t, cudaEvent_t);                                          \
-    template void launch_entropy_batch<T>(const InstTask<T>*, int, cudaStream_t);
+    template void launch_entropy_batch<T>(const InstTask<T>*, int, cudaStream_t);                               \
+    template bool launch_anneal_resident<T>(const InstTask<T>*, const GateOp*, const int*, const int*, int, int, \
+                                            int, int*, int, cudaStream_t);
 TQ_INST(double)
 TQ_INST(float)
 
