@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--jacobi-block", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-solves", action="store_true", help="skip the solves/s (chosen vs plain) measurement")
+    ap.add_argument("--solve-instances", type=int, default=296, help="held-out instances for solves/s")
+    ap.add_argument("--solve-T", type=float, default=10.0, help="anneal time of the solves/s workload")
     ap.add_argument("--profile-run", action="store_true",
                     help="one untimed step only (for ncu); prints no bench line")
     return ap.parse_args()
@@ -67,6 +70,22 @@ def workload(args, rank=0):
     from tessera_b200 import instances
     p = instances.chain_range(n=args.n, dmax=args.dmax, seed=2 + rank, T=50.0, dt=0.02, chi=args.chi)
     return p
+
+
+def shard(rank: int, per_rank: int):
+    """Instance indices of one rank: disjoint contiguous blocks, no data-path exchange."""
+    return [rank * per_rank + b for b in range(per_rank)]
+
+
+def max_over_ranks(ms: float, world: int, device: str = "cuda") -> float:
+    """The step time of the job: the slowest rank's CUDA-event time (all-reduce MAX)."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def peaks():
@@ -227,6 +246,46 @@ def plain_rate(args, local):
     return g / (r.device_ms / 1e3), r.device_ms / g
 
 
+def solves(args):
+    """Second half of the metric: solves/s at <= 1% energy gap, chosen vs plain.
+
+    Dense Erdos-Renyi instances (p = 0.5, J ~ U(-1,1), h ~ U(-0.2,0.2)).  The schedule GNN is
+    trained here, on the GPU, from labels the engine itself generates: 160 training instances
+    n in [8, 12], each annealed under 16 candidate schedules (batched, complex64) and scored by
+    the exact ground energy.  Then on `--solve-instances` held-out instances n in [12, 14]:
+    chosen = learned knots + warm-start bias, batched complex64, with the linear-schedule
+    fallback judged by the engine's own final energy; plain = linear schedule, complex128, one
+    instance per call (timed on 8 instances; energies of all instances from the bit-identical
+    batched complex128 run).  T = --solve-T, dt = 0.1, chi = 32."""
+    from tessera_b200 import instances, learned
+    cfg = learned.LearnConfig(T=args.solve_T, dt=0.1, chi=32, precision="c64")
+    train = [instances.dense_er(n, 1000 + i, T=1.0) for i, n in enumerate(list(range(8, 13)) * 32)]
+    held = [instances.dense_er(n, 50000 + i, T=1.0) for i, n in
+            enumerate(([12, 13, 14] * (args.solve_instances // 3 + 1))[:args.solve_instances])]
+    t0 = time.perf_counter()
+    tk, _, gs, gaps = learned.label(train, cfg, learned.candidates(count=16))
+    t_label = time.perf_counter() - t0
+    net = learned.ScheduleGNN(seed=1)
+    t0 = time.perf_counter()
+    losses = learned.train(net, train, tk, gs, epochs=100, batch=32, lr=2e-3)
+    t_train = time.perf_counter() - t0
+    ev = learned.evaluate(net, held, cfg, plain_sample=8)
+    net.close()
+    return {"metric": "solves/s at <=1% energy gap, chosen vs plain", "unit": "solves/s",
+            "chosen": ev["chosen_solves_per_s"], "plain": ev["plain_solves_per_s"],
+            "ratio": ev["chosen_solves_per_s"] / ev["plain_solves_per_s"] if ev["plain_solves_per_s"] else None,
+            "instances": ev["instances"], "chosen_solved": ev["chosen_solved"], "plain_solved": ev["plain_solved"],
+            "chosen_seconds": ev["chosen_seconds"], "plain_seconds": ev["plain_seconds"],
+            "plain_timed_instances": ev["plain_timed_instances"], "learned_kept": ev["learned_kept"],
+            "chosen_mean_gap": ev["chosen_mean_gap"], "plain_mean_gap": ev["plain_mean_gap"],
+            "train": {"instances": len(train), "candidates": 16, "label_seconds": t_label,
+                      "train_seconds": t_train, "loss_first": losses[0], "loss_last": losses[-1],
+                      "best_candidate_solved": int((gaps.min(axis=1) <= 0.01).sum()),
+                      "linear_solved": int((gaps[:, 0] <= 0.01).sum())},
+            "workload": f"dense ER p=0.5, train n 8..12, held-out n 12..14, T={cfg.T}, dt={cfg.dt}, chi={cfg.chi}; "
+                        "reduced from config 5 (20k train n 8..20, 1024 eval n 24..48, chi=128, T=30)"}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -246,7 +305,7 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     B = max(1, args.batch)
-    probs = [workload(args, rank * B + b) for b in range(B)]
+    probs = [workload(args, i) for i in shard(rank, B)]
     p = probs[0]
     upd_per_step_inst = min(args.gates, p.updates_per_step())
     if B == 1:
@@ -296,10 +355,7 @@ def main():
         dist.barrier()
     ck = clocks.stop()
     ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, world)
     updates = r1.two_site_updates - r0.two_site_updates
     assert updates == B * G * args.steps, (updates, B, G)
     if r1.status:
@@ -376,6 +432,13 @@ def main():
         except Exception as exc:  # the baseline is reported, never required
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {exc}"}
 
+    sol = None
+    if rank == 0 and world == 1 and not args.no_solves:
+        try:
+            sol = solves(args)
+        except Exception as exc:
+            sol = {"value": None, "error": str(exc)}
+
     if rank == 0:
         cfg = config_dict(args, p)
         cfg.update({"instances_per_gpu": B, "gates_per_step": G,
@@ -386,7 +449,7 @@ def main():
                 "data": "synthetic: seeded Ising instances (PCG64 seeds 2..) and seeded random MPS with every "
                         "bond at its cap",
                 "config": cfg, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": launches, "clocks": ck, "plain_single_instance": plain,
+                "gpu_launches": launches, "clocks": ck, "plain_single_instance": plain, "solves": sol,
                 "max_trunc_in_timed_steps": r1.max_trunc}
         print(json.dumps(line))
     if B == 1 or rank != 0:

@@ -96,4 +96,4 @@ def loss_and_grad(params: np.ndarray, problems, target_knots, target_spins, H, L
         q = p[lab].clamp(1e-7, 1 - 1e-7)
         loss = loss + ln * (-(ts[lab] * torch.log(q) + (1 - ts[lab]) * torch.log(1 - q))).mean()
     loss.backward()
-    return float(loss), theta.grad.numpy().copy(), knots.detach().numpy(), p.detach().numpy()
+    return float(loss.detach()), theta.grad.numpy().copy(), knots.detach().numpy(), p.detach().numpy()

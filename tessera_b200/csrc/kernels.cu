@@ -705,16 +705,20 @@ __device__ __forceinline__ void svd_body(const MpsView<T>& mps, const SvdWork<T>
 // so a warp rotates 32/LPP pairs at once and the reduction is log2(LPP) shuffle levels;
 // alpha, beta, gamma are accumulated and reduced in FP64 and the rotation is
 // jacobi_rotation's.  A sweep is N-1 rounds; a sweep without a rotation ends the
-// iteration.  Rows per lane are capped at 8 and LPP grows with R: (LPP, RPL) = (8, R/8)
-// up to R = 64, then (16, 8) and (32, 8).
+// iteration.  Up to 8 register rows per lane (fewer in use for small R) and LPP by size
+// class: 8 up to R = 64, 16 up to 128, 32 up to 256.  One instantiation serves a whole class,
+// so a theta is rotated by the same instructions whatever batch it runs in.
 // ------------------------------------------------------------------------------------
 constexpr int RES_MAXT = 512;
+constexpr int RES_RPL = 8;  // register rows per lane; R <= LPP * RES_RPL
 
-template <typename T, int LPP, int RPL>
+template <typename T, int LPP>
 __device__ void jacobi_core(cplx_t<T>* col, const int rc, const int R, const int N, const double tol,
                             const double tiny, const int max_sweeps, int* s_rot, int& sweeps, bool& converged) {
     using V = cplx_t<T>;
     constexpr int PPW = 32 / LPP;
+    constexpr int RPL = RES_RPL;
+    const int rpl = (R + LPP - 1) / LPP;  // rows per lane in use (<= RPL)
     const int tid = threadIdx.x, NW = blockDim.x >> 5, warp = tid >> 5, lane = tid & 31;
     const int sub = lane / LPP, sl = lane % LPP;
     const int Nc = N + (N & 1);
@@ -740,13 +744,14 @@ __device__ void jacobi_core(cplx_t<T>* col, const int rc, const int R, const int
 #pragma unroll
                 for (int k = 0; k < RPL; ++k) {
                     const int row = sl + LPP * k;
-                    const bool in = ok && row < R;
+                    const bool in = ok && k < rpl && row < R;
                     x[k] = in ? cp[row] : czero<V>();
                     y[k] = in ? cq[row] : czero<V>();
                 }
                 double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
 #pragma unroll
                 for (int k = 0; k < RPL; ++k) {
+                    if (k >= rpl) break;
                     v0 += (double)x[k].x * x[k].x + (double)x[k].y * x[k].y;
                     v1 += (double)y[k].x * y[k].x + (double)y[k].y * y[k].y;
                     v2 += (double)x[k].x * y[k].x + (double)x[k].y * y[k].y;
@@ -763,6 +768,7 @@ __device__ void jacobi_core(cplx_t<T>* col, const int rc, const int R, const int
                 if (ok && jacobi_rotation<T>(v0, v1, v2, v3, tol, tiny, c, sn, er, ei)) {
 #pragma unroll
                     for (int k = 0; k < RPL; ++k) {
+                        if (k >= rpl) break;
                         const int row = sl + LPP * k;
                         const V xv = x[k], yv = y[k];
                         const T ey_re = er * yv.x + ei * yv.y, ey_im = er * yv.y - ei * yv.x;
@@ -843,7 +849,7 @@ __device__ __forceinline__ double noise_tiny(double pp_tiny, int R, double fro2,
     return fmax(pp_tiny, floor_rel * floor_rel * fro2);
 }
 
-template <typename T, int LPP, int RPL>
+template <typename T, int LPP>
 __device__ void svd_resident_body(const MpsView<T>& mps, const SvdWork<T>& wk, const SvdParams& pp,
                                   unsigned char* smraw) {
     using V = cplx_t<T>;
@@ -855,7 +861,7 @@ __device__ void svd_resident_body(const MpsView<T>& mps, const SvdWork<T>& wk, c
     const int N = pp.N > 0 ? pp.N : 2 * mps.dims[pp.bond + 2];
     const int rc = pp.rows_cap;
     V* col = reinterpret_cast<V*>(smraw);  // [cols_cap][rows_cap]
-    if (R > rc || R > LPP * RPL || N > pp.cols_cap) {  // host sizing bug guard
+    if (R > rc || R > LPP * RES_RPL || N > pp.cols_cap) {  // host sizing bug guard
         if (tid == 0) atomicOr(&wk.stats->status, ST_BAD_DIMS);
         return;
     }
@@ -869,19 +875,19 @@ __device__ void svd_resident_body(const MpsView<T>& mps, const SvdWork<T>& wk, c
     const double tiny = noise_tiny(pp.tiny, R, block_fro2<T>(col, rc, R, N, red), sizeof(T) == 4);
     int sweep = 0;
     bool converged = false;
-    jacobi_core<T, LPP, RPL>(col, rc, R, N, pp.tol, tiny, pp.max_sweeps, s_rot, sweep, converged);
+    jacobi_core<T, LPP>(col, rc, R, N, pp.tol, tiny, pp.max_sweeps, s_rot, sweep, converged);
     resident_norms<T>(col, rc, R, N, wk.W, ld, wk.sig2);
     svd_finish<T>(mps, wk, pp, R, N, fmax(1e-28, tiny), sweep, converged, 2.0 * (double)R * N * sizeof(V), smraw,
                   red);
 }
 
-template <typename T, int LPP, int RPL>
+template <typename T, int LPP>
 __global__ void __launch_bounds__(RES_MAXT, 1) k_svd_res(MpsView<T> mps, SvdWork<T> wk, SvdParams pp) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    svd_resident_body<T, LPP, RPL>(mps, wk, pp, smraw);
+    svd_resident_body<T, LPP>(mps, wk, pp, smraw);
 }
 
-template <typename T, int LPP, int RPL>
+template <typename T, int LPP>
 __global__ void __launch_bounds__(RES_MAXT, 1) k_svd_res_batch(const InstTask<T>* insts, const UpdRef* refs,
                                                               int nref) {
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -890,7 +896,7 @@ __global__ void __launch_bounds__(RES_MAXT, 1) k_svd_res_batch(const InstTask<T>
         const InstTask<T>& it = insts[rf.inst];
         SvdParams pp = it.pp;
         pp.bond = rf.op.bond;
-        svd_resident_body<T, LPP, RPL>(it.mps, it.wk, pp, smraw);
+        svd_resident_body<T, LPP>(it.mps, it.wk, pp, smraw);
         __syncthreads();
     }
 }
@@ -910,7 +916,7 @@ __device__ void entropy_body(const MpsView<T>& mps, const cplx_t<T>* r1, double*
 // so instances never wait for the slowest SVD of a gate slot and the whole run is one
 // launch.  256 threads (the environment GEMMs of the entropy step use 256).
 // ------------------------------------------------------------------------------------
-template <typename T, int LPP, int RPL>
+template <typename T, int LPP>
 __device__ void resident_update(const MpsView<T>& mps, const ScheduleView& sch, const GateOp& op,
                                 const SvdWork<T>& wk, const SvdParams& pp0, cplx_t<T>* col, unsigned char* sortbuf,
                                 double* red, int* s_rot) {
@@ -919,7 +925,7 @@ __device__ void resident_update(const MpsView<T>& mps, const ScheduleView& sch, 
     const int i = op.bond;
     const int dl = mps.dims[i], mid = mps.dims[i + 1], dr = mps.dims[i + 2];
     const int R = 2 * dl, N = 2 * dr, rc = pp0.rows_cap, ld = wk.ld, cap = mps.cap;
-    if (R > rc || R > LPP * RPL || N > pp0.cols_cap) {
+    if (R > rc || R > LPP * RES_RPL || N > pp0.cols_cap) {
         if (tid == 0) atomicOr(&wk.stats->status, ST_BAD_DIMS);
         return;
     }
@@ -961,7 +967,7 @@ __device__ void resident_update(const MpsView<T>& mps, const ScheduleView& sch, 
     const double tiny = noise_tiny(pp0.tiny, R, block_fro2<T>(col, rc, R, N, red), sizeof(T) == 4);
     int sweep = 0;
     bool converged = false;
-    jacobi_core<T, LPP, RPL>(col, rc, R, N, pp0.tol, tiny, pp0.max_sweeps, s_rot, sweep, converged);
+    jacobi_core<T, LPP>(col, rc, R, N, pp0.tol, tiny, pp0.max_sweeps, s_rot, sweep, converged);
     resident_norms<T>(col, rc, R, N, nullptr, ld, wk.sig2);
     SvdParams pp = pp0;
     pp.bond = i;
@@ -997,7 +1003,7 @@ __device__ void resident_update(const MpsView<T>& mps, const ScheduleView& sch, 
     __syncthreads();
 }
 
-template <typename T, int LPP, int RPL>
+template <typename T, int LPP>
 __global__ void __launch_bounds__(256) k_anneal_res(const InstTask<T>* insts, const GateOp* ops, const int* op_off,
                                                     const int* order, int ninst, int k0, int k1, int* work,
                                                     size_t col_bytes) {
@@ -1027,7 +1033,7 @@ __global__ void __launch_bounds__(256) k_anneal_res(const InstTask<T>* insts, co
             for (int i = 0; i < mps.n; ++i) single_site_body<T>(mps, sch, i, 0, 1);
             __syncthreads();
             for (int q = q0; q < q1; ++q)
-                resident_update<T, LPP, RPL>(mps, sch, ops[q], it.wk, it.pp, col, sortbuf, red, s_rot);
+                resident_update<T, LPP>(mps, sch, ops[q], it.wk, it.pp, col, sortbuf, red, s_rot);
             for (int i = 0; i < mps.n; ++i) single_site_body<T>(mps, sch, i, 0, 1);
             __syncthreads();
             if (mps.n >= 2) {
@@ -1054,30 +1060,24 @@ static size_t resident_smem(int rows_cap, int cols_cap, bool with_cols = false) 
     return (rows_cap <= 256 && b <= 200 * 1024) ? b : 0;
 }
 
-// (LPP, RPL) for a row count: the index of the smallest shape with LPP RPL >= rows_cap
-static int resident_shape(int rows_cap) {
-    if (rows_cap <= 8) return 0;
-    if (rows_cap <= 16) return 1;
-    if (rows_cap <= 32) return 2;
-    if (rows_cap <= 64) return 3;
-    if (rows_cap <= 128) return 4;
-    if (rows_cap <= 256) return 5;
-    return -1;
+// lanes per pair for a row count: the size class (8 lanes up to 64 rows, 16 up to 128, 32 up to 256)
+static int resident_lpp(int rows_cap) {
+    if (rows_cap <= 8 * RES_RPL) return 8;
+    if (rows_cap <= 16 * RES_RPL) return 16;
+    if (rows_cap <= 32 * RES_RPL) return 32;
+    return 0;
 }
 
-#define TQ_RES_SHAPES(F)             \
-    switch (resident_shape(pp.rows_cap)) { \
-        case 0: F(8, 1); break;       \
-        case 1: F(8, 2); break;       \
-        case 2: F(8, 4); break;       \
-        case 3: F(8, 8); break;       \
-        case 4: F(16, 8); break;      \
-        case 5: F(32, 8); break;      \
-        default: return false;        \
+#define TQ_RES_SHAPES(F)                     \
+    switch (resident_lpp(pp.rows_cap)) {     \
+        case 8: F(8); break;                 \
+        case 16: F(16); break;               \
+        case 32: F(32); break;               \
+        default: return false;               \
     }
 
 // Launch one resident-Jacobi kernel (single theta when insts == nullptr, else a batch).
-template <typename T, int LPP, int RPL>
+template <typename T, int LPP>
 static void res_launch(const MpsView<T>* mps, const SvdWork<T>* wk, const SvdParams& pp, const InstTask<T>* insts,
                        const UpdRef* refs, int nref, cudaStream_t s) {
     const size_t smem = resident_smem<T>(pp.rows_cap, pp.cols_cap);
@@ -1086,7 +1086,7 @@ static void res_launch(const MpsView<T>* mps, const SvdWork<T>* wk, const SvdPar
     int nt = 32 * (warps < 1 ? 1 : warps);
     if (nt > RES_MAXT) nt = RES_MAXT;
     if (insts) {
-        auto fn = k_svd_res_batch<T, LPP, RPL>;
+        auto fn = k_svd_res_batch<T, LPP>;
         TQ_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
         TQ_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, nt, smem));
@@ -1095,7 +1095,7 @@ static void res_launch(const MpsView<T>* mps, const SvdWork<T>* wk, const SvdPar
         if (grid > nref) grid = nref;
         fn<<<grid, nt, smem, s>>>(insts, refs, nref);
     } else {
-        auto fn = k_svd_res<T, LPP, RPL>;
+        auto fn = k_svd_res<T, LPP>;
         TQ_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         fn<<<1, nt, smem, s>>>(*mps, *wk, pp);
     }
@@ -1106,18 +1106,18 @@ template <typename T>
 static bool res_dispatch(const MpsView<T>* mps, const SvdWork<T>* wk, const SvdParams& pp, const InstTask<T>* insts,
                          const UpdRef* refs, int nref, cudaStream_t s) {
     if (!resident_smem<T>(pp.rows_cap, pp.cols_cap)) return false;
-#define TQ_F(L, RP) res_launch<T, L, RP>(mps, wk, pp, insts, refs, nref, s)
+#define TQ_F(L) res_launch<T, L>(mps, wk, pp, insts, refs, nref, s)
     TQ_RES_SHAPES(TQ_F)
 #undef TQ_F
     return true;
 }
 
-template <typename T, int LPP, int RPL>
+template <typename T, int LPP>
 static void anneal_res_launch(const InstTask<T>* insts, const GateOp* ops, const int* op_off, const int* order,
                               int ninst, int k0, int k1, int* work, int rows_cap, cudaStream_t s) {
     const size_t smem = resident_smem<T>(rows_cap, rows_cap, true);
     const size_t col_bytes = (sizeof(cplx_t<T>) * (size_t)rows_cap * rows_cap + 15) & ~(size_t)15;
-    auto fn = k_anneal_res<T, LPP, RPL>;
+    auto fn = k_anneal_res<T, LPP>;
     TQ_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     TQ_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, smem));
@@ -1135,7 +1135,7 @@ bool launch_anneal_resident(const InstTask<T>* insts, const GateOp* ops, const i
     if (!resident_smem<T>(rows_cap, rows_cap, true)) return false;
     SvdParams pp{};
     pp.rows_cap = rows_cap;
-#define TQ_F(L, RP) anneal_res_launch<T, L, RP>(insts, ops, op_off, order, ninst, k0, k1, work, rows_cap, s)
+#define TQ_F(L) anneal_res_launch<T, L>(insts, ops, op_off, order, ninst, k0, k1, work, rows_cap, s)
     TQ_RES_SHAPES(TQ_F)
 #undef TQ_F
     return true;

@@ -200,6 +200,12 @@ def with_schedule(p: instances.Problem, knots, cfg: LearnConfig, bias=None) -> i
     return q
 
 
+def plain_problem(p: instances.Problem, cfg: LearnConfig) -> instances.Problem:
+    """The plain method: the linear schedule A = 1 - s, B = s (rust/src/schedule.rs:20-31), no bias."""
+    sa, sb = instances.linear(int(round(cfg.T / cfg.dt)))
+    return instances.Problem(p.h, p.ei, p.ej, p.ew, sa, sb, cfg.dt, cfg.chi, p.name)
+
+
 def label(problems, cfg: LearnConfig, cands=None, chunk: int = 512):
     """Best candidate schedule (lowest readout energy, then lowest <H>) per problem, and the exact
     ground state.  Returns (target knots (G, K), ground energies, ground spins list, gaps per candidate)."""
@@ -246,9 +252,8 @@ def solve_chosen(gnn: ScheduleGNN, problems, cfg: LearnConfig, use_bias=True):
     """Learned schedule (+ warm-start bias) and the plain linear schedule in one batch; per problem
     keep the run whose readout energy is lower (fallback to linear when the learned run is worse)."""
     kn, bias = gnn.predict(problems)
-    lin = np.linspace(0.0, 1.0, gnn.knots)
     runs = [with_schedule(p, kn[g], cfg, bias[g] if use_bias else None) for g, p in enumerate(problems)]
-    runs += [with_schedule(p, lin, cfg) for p in problems]
+    runs += [plain_problem(p, cfg) for p in problems]
     res = ffi.anneal_batch(runs, precision=cfg.precision, raise_on_status=False)
     G = len(problems)
     out = []
@@ -259,28 +264,44 @@ def solve_chosen(gnn: ScheduleGNN, problems, cfg: LearnConfig, use_bias=True):
     return out
 
 
-def evaluate(gnn: ScheduleGNN, problems, cfg: LearnConfig, gap=0.01):
+def evaluate(gnn: ScheduleGNN, problems, cfg: LearnConfig, gap=0.01, plain_sample: int | None = None):
     """Solves per second, chosen (batched c64, learned + fallback) vs plain (c128, one instance at
-    a time, linear schedule), on the same problems; ground energies from tessera_qa_exact_ground."""
+    a time, linear schedule), on the same problems; ground energies from tessera_qa_exact_ground.
+
+    plain_sample = k: the plain arm is timed on the first k problems, one call each, and its
+    per-instance time is taken as their mean; its energies for all problems come from one
+    batched complex128 run of the same linear schedule, which executes the same per-instance
+    code (the resident anneal kernel) and gives the same results -- checked on the timed
+    sample."""
     e0 = np.array([exact_ground(p)[0] for p in problems])
     steps = int(round(cfg.T / cfg.dt))
+    sa, sb = instances.linear(steps)
+    timed = problems if plain_sample is None else problems[:plain_sample]
     t0 = time.perf_counter()
-    plain_e = []
-    for p in problems:
-        sa, sb = instances.linear(steps)
+    single_e = []
+    for p in timed:
         r = ffi.anneal(p.h, p.ei, p.ej, p.ew, sa, sb, dt=cfg.dt, chi=cfg.chi, precision="c128",
                        raise_on_status=False)
-        plain_e.append(r.energy)
-    t_plain = time.perf_counter() - t0
+        single_e.append(r.energy)
+    t_timed = time.perf_counter() - t0
+    if plain_sample is None:
+        plain_e = np.array(single_e)
+        t_plain = t_timed
+    else:
+        res = ffi.anneal_batch([plain_problem(p, cfg) for p in problems], precision="c128", raise_on_status=False)
+        plain_e = np.array([r.energy for r in res])
+        if not np.array_equal(plain_e[:len(timed)], np.array(single_e)):
+            raise RuntimeError("batched complex128 plain runs differ from the single-instance runs")
+        t_plain = t_timed / max(1, len(timed)) * len(problems)
     t0 = time.perf_counter()
     ch = solve_chosen(gnn, problems, cfg)
     t_chosen = time.perf_counter() - t0
     chosen_e = np.array([c[0] for c in ch])
-    plain_e = np.array(plain_e)
     ok_plain = (plain_e - e0) / np.abs(e0) <= gap
     ok_chosen = (chosen_e - e0) / np.abs(e0) <= gap
     return {"instances": len(problems), "plain_solved": int(ok_plain.sum()), "chosen_solved": int(ok_chosen.sum()),
             "plain_seconds": t_plain, "chosen_seconds": t_chosen,
+            "plain_timed_instances": len(timed),
             "plain_solves_per_s": ok_plain.sum() / t_plain, "chosen_solves_per_s": ok_chosen.sum() / t_chosen,
             "learned_kept": int(sum(c[1] for c in ch)),
             "plain_mean_gap": float(np.mean((plain_e - e0) / np.abs(e0))),

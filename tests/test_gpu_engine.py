@@ -233,19 +233,20 @@ def test_chain16_chi32_against_statevector(oracle):
 
 def test_batched_anneal_equals_single_instance_runs():
     """tessera_qa_anneal_batch: ragged instances (different n, edges, chi) give the same results as
-    one tessera_qa_anneal_ex call each."""
+    one tessera_qa_anneal_ex call each.  With every theta of at most 64 rows both run the same
+    resident anneal kernel for each instance, so the results are bit for bit equal."""
     probs = [instances.chain_range(n=8, dmax=2, seed=5, T=2.0, dt=0.05, chi=4, dist="normal", hzero=False),
              instances.chain_range(n=10, dmax=3, seed=6, T=2.0, dt=0.05, chi=8, dist="normal", hzero=False),
              instances.chain_nn(n=12, seed=7, T=2.0, dt=0.05, chi=16),
              instances.dense_er(n=7, seed=8, T=2.0, dt=0.05, chi=8)]
-    for prec, tol in (("c128", 1e-9), ("c64", 1e-4)):
+    for prec in ("c128", "c64"):
         batch = ffi.anneal_batch(probs, precision=prec)
         for p, rb in zip(probs, batch):
             rs = ffi.anneal(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=p.chi, precision=prec)
             assert rb.two_site_updates == rs.two_site_updates
-            assert rb.expected_energy == pytest.approx(rs.expected_energy, rel=tol, abs=tol), (p.name, prec)
-            assert np.max(np.abs(rb.entropy - rs.entropy)) < tol * 10, (p.name, prec)
-            assert spins_agree(rb, rs.spins)
+            assert rb.expected_energy == rs.expected_energy, (p.name, prec)
+            assert np.array_equal(rb.entropy, rs.entropy), (p.name, prec)
+            assert list(rb.spins) == list(rs.spins) and rb.max_trunc == rs.max_trunc
             assert rb.status == 0
 
 
