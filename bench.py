@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--solve-T", type=float, default=10.0, help="anneal time of the solves/s workload")
     ap.add_argument("--profile-run", action="store_true",
                     help="one untimed step only (for ncu); prints no bench line")
+    ap.add_argument("--profile-anneal", action="store_true",
+                    help="one batched anneal of 148 dense ER instances n=12, chi=32, T=1 (the small-bond resident "
+                         "kernel, for ncu); prints no bench line")
     return ap.parse_args()
 
 
@@ -286,10 +289,21 @@ def solves(args):
                         "reduced from config 5 (20k train n 8..20, 1024 eval n 24..48, chi=128, T=30)"}
 
 
+def profile_anneal():
+    from tessera_b200 import ffi, instances
+    probs = [instances.dense_er(12, 100 + i, T=1.0, dt=0.1, chi=32) for i in range(148)]
+    res = ffi.anneal_batch(probs, precision="c64", raise_on_status=False)
+    print(f"profile anneal: {sum(r.two_site_updates for r in res)} updates, status "
+          f"{sorted(set(r.status for r in res))}, {res[0].device_ms:.1f} ms")
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.profile_anneal:
+        profile_anneal()
         return
     import numpy as np
     import torch

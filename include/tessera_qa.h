@@ -239,6 +239,8 @@ TESSERA_QA_API int tessera_qa_session_observe(tessera_qa_session* s, tessera_qa_
 /* Writes / reads a checkpoint of the current state. */
 TESSERA_QA_API int tessera_qa_session_save(tessera_qa_session* s, void* buf, size_t bytes);
 TESSERA_QA_API int tessera_qa_session_load(tessera_qa_session* s, const void* buf, size_t bytes);
+/* Checkpoint of one instance of a batched session (index 0 for a single-instance session). */
+TESSERA_QA_API int tessera_qa_session_save_instance(tessera_qa_session* s, size_t index, void* buf, size_t bytes);
 TESSERA_QA_API void tessera_qa_session_destroy(tessera_qa_session* s);
 
 #ifdef __cplusplus

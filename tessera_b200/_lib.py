@@ -106,6 +106,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.tessera_qa_session_save.restype = C.c_int
         L.tessera_qa_session_load.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
         L.tessera_qa_session_load.restype = C.c_int
+        L.tessera_qa_session_save_instance.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t]
+        L.tessera_qa_session_save_instance.restype = C.c_int
         L.tessera_qa_session_destroy.argtypes = [C.c_void_p]
         L.tessera_qa_session_destroy.restype = None
         _lib = L

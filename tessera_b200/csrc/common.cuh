@@ -156,6 +156,12 @@ __device__ __forceinline__ void fence_proxy_async_global() {
     asm volatile("fence.proxy.async.global;" ::: "memory");
 }
 
+// Orders this thread's generic-proxy shared-memory accesses before async-proxy (TMA) writes
+// into the same buffer that it issues after the fence.
+__device__ __forceinline__ void fence_proxy_async_shared() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 // Warp-level sum with shuffles.
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll

@@ -809,6 +809,7 @@ public:
     virtual void set_values(const std::vector<ProblemHost>& P) = 0;
     virtual void sync(tessera_qa_result* r) = 0;  // aggregated over the instances
     virtual cudaStream_t stream() const = 0;
+    virtual void save(int b, void* buf, size_t bytes) = 0;  // checkpoint of instance b
 };
 
 template <typename T>
@@ -825,7 +826,7 @@ public:
             q_max_ = std::max(q_max_, (int)eng_.back()->ops().size());
         }
         steps_ = steps;
-        block_ = C[0].block ? C[0].block : (2 * cap_max_ <= 64 ? 16 : 8);
+        block_ = C[0].block;  // 0: resident or block-Gram Jacobi by size; else column-pair blocks of this width
         rows_cap_ = std::max(8, (2 * cap_max_ + 7) & ~7);
         TQ_CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
         TQ_CK(cudaEventCreate(&e0_));
@@ -890,6 +891,11 @@ public:
     }
     int size() const override { return (int)eng_.size(); }
     Engine<T>& at(int b) { return *eng_[b]; }
+    void save(int b, void* buf, size_t bytes) override {
+        if (b < 0 || b >= (int)eng_.size()) throw ArgError("instance index out of range");
+        TQ_CK(cudaStreamSynchronize(st_));
+        eng_[b]->save(buf, bytes, 0);
+    }
     cudaStream_t stream() const override { return st_; }
     void set_timing(bool on) { timing_ = on; }
 
@@ -1395,6 +1401,19 @@ int tessera_qa_session_save(tessera_qa_session* s, void* buf, size_t bytes) {
         if (!s) throw ArgError("session is NULL");
         if (s->batch) throw ArgError("checkpoints are per instance");
         s->eng->save(buf, bytes, 0);
+        return 0;
+    });
+}
+
+int tessera_qa_session_save_instance(tessera_qa_session* s, size_t index, void* buf, size_t bytes) {
+    return guarded([&]() -> int {
+        if (!s) throw ArgError("session is NULL");
+        if (s->batch) {
+            s->batch->save((int)std::min<size_t>(index, 1u << 30), buf, bytes);
+        } else {
+            if (index != 0) throw ArgError("instance index out of range");
+            s->eng->save(buf, bytes, 0);
+        }
         return 0;
     });
 }

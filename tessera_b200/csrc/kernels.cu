@@ -1141,6 +1141,354 @@ bool launch_anneal_resident(const InstTask<T>* insts, const GateOp* ops, const i
     return true;
 }
 
+// ------------------------------------------------------------------------------------
+// K2g: block-Gram one-sided Jacobi for large theta, one CTA per theta (the batched path).
+// Columns are cut into blocks of BG_B = 32; a round-robin tournament over the P blocks gives
+// P-1 rounds of P/2 block pairs per sweep, all taken by the one CTA in turn.  For a block
+// pair (64 columns Wp) the CTA
+//   1. forms the 64 x 64 Gram matrix G = Wp^H Wp in FP64 from row chunks of the 64 columns,
+//      streamed into shared memory by 1-D TMA bulk copies (two buffers: the copy of chunk
+//      k+1 runs under the arithmetic on chunk k);
+//   2. runs one cyclic sweep of two-sided Jacobi on G (circle method, 32 disjoint rotations
+//      per round, each from jacobi_rotation on (G_pp, G_qq, G_pq): the rotation the
+//      column-pair kernel would compute from the same dot products), accumulating the
+//      64 x 64 unitary V;
+//   3. applies Wp <- Wp V over the row chunks (a GEMM) -- skipped when nothing rotated.
+// The convergence test is FP64 on every pair of a freshly formed Gram matrix; a sweep in
+// which no block pair rotates ends the iteration.  Per sweep the columns are read twice and
+// written once per block pair: (P-1) (2 + 1) column passes for P = N/32 blocks, against
+// 2 (P-1) passes of 8-column blocks (P = N/8) in the column-pair kernel, and the arithmetic
+// is two GEMMs per block pair instead of one shuffle reduction and one barrier per pair.
+// ------------------------------------------------------------------------------------
+constexpr int BG_B = 32;
+constexpr int BG_W = 2 * BG_B;  // columns of a block pair
+constexpr int BG_RC = 32;       // rows per streamed chunk
+constexpr int BG_NT = 256;
+constexpr int BG_GS = BG_W + 1;  // padded row stride of G and V (double2 elements)
+
+template <typename T>
+struct BgShape {
+    // padded column stride of a chunk (elements): odd for 16-byte elements (bank spread),
+    // even for 8-byte ones (16-byte aligned TMA destinations)
+    static constexpr int CS = sizeof(T) == 8 ? BG_RC + 1 : BG_RC + 2;
+    static constexpr size_t g_bytes = sizeof(double2) * BG_W * BG_GS;
+    static constexpr size_t chunk_bytes = ((sizeof(cplx_t<T>) * BG_W * CS + 127) / 128) * 128;
+    static constexpr size_t smem = 2 * g_bytes + 2 * chunk_bytes;
+};
+
+struct BgRot {
+    double c, s, er, ei;
+    int p, q, act, pad;
+};
+
+template <typename T>
+__device__ __forceinline__ int bg_col(int c, int I, int J, int N) {
+    const int g = c < BG_B ? I * BG_B + c : J * BG_B + (c - BG_B);
+    return g < N ? g : -1;
+}
+
+// Stage rows [r0, r0 + BG_RC) of the pair's 64 columns into `ch` (column c at c * CS):
+// thread 0 issues one bulk copy per valid column; all threads zero the rest.
+template <typename T>
+__device__ __forceinline__ void bg_stage(cplx_t<T>* ch, const cplx_t<T>* W, int ld, int R, int N, int I, int J,
+                                         int r0, uint64_t* bar) {
+    using V = cplx_t<T>;
+    constexpr int CS = BgShape<T>::CS;
+    const int rows = R - r0 < BG_RC ? R - r0 : BG_RC;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < BG_W * BG_RC; e += BG_NT) {
+        const int c = e / BG_RC, r = e - c * BG_RC;
+        if (bg_col<T>(c, I, J, N) < 0 || r >= rows) ch[c * CS + r] = czero<V>();
+    }
+    if (tid == 0) {
+        unsigned nv = 0;
+        for (int c = 0; c < BG_W; ++c) nv += bg_col<T>(c, I, J, N) >= 0;
+        const unsigned bytes = (unsigned)(rows * sizeof(V));
+        fence_proxy_async_shared();
+        mbar_expect_tx(bar, nv * bytes);
+        for (int c = 0; c < BG_W; ++c) {
+            const int g = bg_col<T>(c, I, J, N);
+            if (g >= 0) tma_load_1d(ch + c * CS, W + (long long)g * ld + r0, bytes, bar);
+        }
+    }
+}
+
+// Wait for a staged chunk with one CTA-wide decision: thread 0 waits (bounded) and
+// publishes the outcome, every thread then re-checks the completed phase (bounded, returns
+// at once) so that its own reads of the buffer are ordered after the copies.
+__device__ __forceinline__ bool bg_wait(uint64_t* bar, unsigned& ph, int* s_ok) {
+    if (threadIdx.x == 0) *s_ok = mbar_wait(bar, ph, 1000000000ull) ? 1 : 0;
+    __syncthreads();
+    const bool ok = *s_ok != 0;
+    if (ok && threadIdx.x != 0) mbar_wait(bar, ph, 1000000000ull);
+    if (ok) ph ^= 1u;
+    return ok;
+}
+
+// One block pair: Gram, one Jacobi sweep on it, apply.  Returns false (on every thread) when
+// a copy did not complete within its time budget.
+template <typename T>
+__device__ bool bg_pair(const SvdWork<T>& wk, int R, int N, int I, int J, double tol, double tiny, double2* G,
+                        double2* Vm, cplx_t<T>* ch0, cplx_t<T>* ch1, uint64_t* bars, unsigned* phase, BgRot* prm,
+                        int* s_rot, double* bytes) {
+    using V = cplx_t<T>;
+    constexpr int CS = BgShape<T>::CS;
+    const int tid = threadIdx.x;
+    const int ld = wk.ld;
+    V* W = wk.W;
+    V* ch[2] = {ch0, ch1};
+    const int nchunk = (R + BG_RC - 1) / BG_RC;
+    int nvalid = 0;
+    for (int c = 0; c < BG_W; ++c) nvalid += bg_col<T>(c, I, J, N) >= 0;
+    // ---- 1. Gram: thread (ti, tj) owns G[ti + 16k][tj + 16l], k, l < 4 ----
+    const int ti = tid >> 4, tj = tid & 15;
+    double2 acc[4][4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int l = 0; l < 4; ++l) acc[k][l] = make_double2(0.0, 0.0);
+    bg_stage<T>(ch[0], W, ld, R, N, I, J, 0, &bars[0]);
+    for (int kc = 0; kc < nchunk; ++kc) {
+        const int b = kc & 1;
+        if (kc + 1 < nchunk) bg_stage<T>(ch[b ^ 1], W, ld, R, N, I, J, (kc + 1) * BG_RC, &bars[b ^ 1]);
+        if (!bg_wait(&bars[b], phase[b], &s_rot[2])) return false;  // (its barrier also publishes the zero fills)
+        const V* cb = ch[b];
+#pragma unroll 2
+        for (int r = 0; r < BG_RC; ++r) {
+            V a[4], y[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                a[k] = cb[(ti + 16 * k) * CS + r];
+                y[k] = cb[(tj + 16 * k) * CS + r];
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int l = 0; l < 4; ++l) {
+                    const double ax = a[k].x, ay = a[k].y, bx = y[l].x, by = y[l].y;
+                    acc[k][l].x = fma(ax, bx, fma(ay, by, acc[k][l].x));
+                    acc[k][l].y = fma(ax, by, fma(-ay, bx, acc[k][l].y));
+                }
+        }
+        __syncthreads();  // buffer b free for the copy after next
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int l = 0; l < 4; ++l) G[(ti + 16 * k) * BG_GS + tj + 16 * l] = acc[k][l];
+    for (int e = tid; e < BG_W * BG_W; e += BG_NT) {
+        const int i = e / BG_W, j = e - i * BG_W;
+        Vm[i * BG_GS + j] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+    }
+    if (tid == 0) s_rot[1] = 0;
+    __syncthreads();
+    *bytes += (double)nvalid * R * sizeof(V);
+    // ---- 2. one cyclic two-sided Jacobi sweep on G, V accumulated ----
+    for (int rd = 0; rd < BG_W - 1; ++rd) {
+        if (tid < BG_W / 2) {
+            int p, q;
+            tournament(BG_W, rd, tid, p, q);
+            BgRot t;
+            t.p = p;
+            t.q = q;
+            const double2 gpq = G[p * BG_GS + q];
+            t.act = jacobi_rotation<double>(G[p * BG_GS + p].x, G[q * BG_GS + q].x, gpq.x, gpq.y, tol, tiny, t.c, t.s,
+                                            t.er, t.ei)
+                        ? 1
+                        : 0;
+            prm[tid] = t;
+            if (t.act) atomicAdd(&s_rot[1], 1);
+        }
+        __syncthreads();
+        // columns p, q of G and V:  x' = c x - s conj(e) y,  y' = s e x + c y
+        for (int e = tid; e < 2 * BG_W * (BG_W / 2); e += BG_NT) {
+            const int m = e / (BG_W * (BG_W / 2));
+            const int rem = e - m * (BG_W * (BG_W / 2));
+            const int k = rem / BG_W, row = rem - k * BG_W;
+            const BgRot t = prm[k];
+            if (!t.act) continue;
+            double2* M = m ? Vm : G;
+            const double2 x = M[row * BG_GS + t.p], y = M[row * BG_GS + t.q];
+            const double ey_re = t.er * y.x + t.ei * y.y, ey_im = t.er * y.y - t.ei * y.x;
+            const double ex_re = t.er * x.x - t.ei * x.y, ex_im = t.er * x.y + t.ei * x.x;
+            M[row * BG_GS + t.p] = make_double2(t.c * x.x - t.s * ey_re, t.c * x.y - t.s * ey_im);
+            M[row * BG_GS + t.q] = make_double2(t.s * ex_re + t.c * y.x, t.s * ex_im + t.c * y.y);
+        }
+        __syncthreads();
+        // rows p, q of G:  x' = c x - s e y,  y' = s conj(e) x + c y
+        for (int e = tid; e < BG_W * (BG_W / 2); e += BG_NT) {
+            const int k = e / BG_W, col = e - k * BG_W;
+            const BgRot t = prm[k];
+            if (!t.act) continue;
+            const double2 x = G[t.p * BG_GS + col], y = G[t.q * BG_GS + col];
+            const double ey_re = t.er * y.x - t.ei * y.y, ey_im = t.er * y.y + t.ei * y.x;
+            const double ex_re = t.er * x.x + t.ei * x.y, ex_im = t.er * x.y - t.ei * x.x;
+            G[t.p * BG_GS + col] = make_double2(t.c * x.x - t.s * ey_re, t.c * x.y - t.s * ey_im);
+            G[t.q * BG_GS + col] = make_double2(t.s * ex_re + t.c * y.x, t.s * ex_im + t.c * y.y);
+        }
+        __syncthreads();
+    }
+    const int nrot = s_rot[1];
+    if (nrot == 0) return true;
+    if (tid == 0) s_rot[0] += nrot;
+    // ---- 3. Wp <- Wp V: thread (tr, tc) owns chunk row tr, columns tc + 8m ----
+    const int tr = tid & 31, tc = tid >> 5;
+    bg_stage<T>(ch[0], W, ld, R, N, I, J, 0, &bars[0]);
+    for (int kc = 0; kc < nchunk; ++kc) {
+        const int b = kc & 1;
+        if (kc + 1 < nchunk) bg_stage<T>(ch[b ^ 1], W, ld, R, N, I, J, (kc + 1) * BG_RC, &bars[b ^ 1]);
+        if (!bg_wait(&bars[b], phase[b], &s_rot[2])) return false;
+        const V* cb = ch[b];
+        double2 o[8];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) o[m] = make_double2(0.0, 0.0);
+        for (int k = 0; k < BG_W; ++k) {
+            const V w = cb[k * CS + tr];
+            const double wx = w.x, wy = w.y;
+#pragma unroll
+            for (int m = 0; m < 8; ++m) {
+                const double2 v = Vm[k * BG_GS + tc + 8 * m];
+                o[m].x = fma(wx, v.x, fma(-wy, v.y, o[m].x));
+                o[m].y = fma(wx, v.y, fma(wy, v.x, o[m].y));
+            }
+        }
+        const int row = kc * BG_RC + tr;
+        if (row < R)
+#pragma unroll
+            for (int m = 0; m < 8; ++m) {
+                const int g = bg_col<T>(tc + 8 * m, I, J, N);
+                if (g >= 0) W[(long long)g * ld + row] = mk<V>((T)o[m].x, (T)o[m].y);
+            }
+        __syncthreads();
+    }
+    // the next block pair's bulk copies read what these stores wrote
+    fence_proxy_async_global();
+    __syncthreads();
+    *bytes += 2.0 * (double)nvalid * R * sizeof(V);
+    return true;
+}
+
+template <typename T>
+__device__ void svd_bgj_body(const MpsView<T>& mps, const SvdWork<T>& wk, const SvdParams& pp, unsigned char* smraw) {
+    using V = cplx_t<T>;
+    __shared__ double red[4 * (BG_NT / 32)];
+    __shared__ int s_rot[3];  // [0] rotations this sweep, [1] this block pair, [2] copy-wait outcome
+    __shared__ BgRot prm[BG_W / 2];
+    __shared__ __align__(8) uint64_t bars[2];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    constexpr int NW = BG_NT / 32;
+    const int R = pp.R > 0 ? pp.R : 2 * mps.dims[pp.bond];
+    const int N = pp.N > 0 ? pp.N : 2 * mps.dims[pp.bond + 2];
+    int* status = &wk.stats->status;
+    double2* G = reinterpret_cast<double2*>(smraw);
+    double2* Vm = G + BG_W * BG_GS;
+    V* ch0 = reinterpret_cast<V*>(smraw + 2 * BgShape<T>::g_bytes);
+    V* ch1 = reinterpret_cast<V*>(smraw + 2 * BgShape<T>::g_bytes + BgShape<T>::chunk_bytes);
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+    }
+    unsigned phase[2] = {0u, 0u};
+    // ||W||_F^2 for the noise floor
+    double part = 0.0;
+    for (int j = warp; j < N; j += NW) {
+        const V* w = wk.W + (long long)j * wk.ld;
+        double sj = 0.0;
+        for (int row = lane; row < R; row += 32) sj += (double)w[row].x * w[row].x + (double)w[row].y * w[row].y;
+        part += warp_sum(sj);
+    }
+    if (lane == 0) red[warp] = part;
+    __syncthreads();
+    double fro2 = 0.0;
+    for (int w = 0; w < NW; ++w) fro2 += red[w];
+    const double tiny = noise_tiny(pp.tiny, R, fro2, sizeof(T) == 4);
+    __syncthreads();
+    const int nb = (N + BG_B - 1) / BG_B;
+    const int P = nb + (nb & 1);
+    double bytes = (double)R * N * sizeof(V);
+    int sweep = 0;
+    bool converged = false;
+    for (; sweep < pp.max_sweeps; ++sweep) {
+        if (tid == 0) s_rot[0] = 0;
+        __syncthreads();
+        for (int r = 0; r < P - 1; ++r)
+            for (int pr = 0; pr < P / 2; ++pr) {
+                int I, J;
+                tournament(P, r, pr, I, J);
+                if (!bg_pair<T>(wk, R, N, I, J, pp.tol, tiny, G, Vm, ch0, ch1, bars, phase, prm, s_rot, &bytes)) {
+                    // every thread leaves here together; wait (bounded) for the copies still in
+                    // flight so that none lands in shared memory after the CTA has moved on
+                    if (tid == 0) {
+                        atomicOr(status, ST_BARRIER_TIMEOUT);
+                        mbar_wait(&bars[0], phase[0], 1000000000ull);
+                        mbar_wait(&bars[1], phase[1], 1000000000ull);
+                    }
+                    __syncthreads();
+                    return;
+                }
+            }
+        __syncthreads();
+        const int done = s_rot[0];
+        __syncthreads();
+        if (done == 0) {
+            converged = true;
+            ++sweep;
+            break;
+        }
+    }
+    // column norms -> sig2 (FP64)
+    for (int j = warp; j < N; j += NW) {
+        const V* w = wk.W + (long long)j * wk.ld;
+        double sj = 0.0;
+        for (int row = lane; row < R; row += 32) sj += (double)w[row].x * w[row].x + (double)w[row].y * w[row].y;
+        sj = warp_sum(sj);
+        if (lane == 0) wk.sig2[j] = sj;
+    }
+    __syncthreads();
+    bytes += (double)R * N * sizeof(V);
+    svd_finish<T>(mps, wk, pp, R, N, fmax(1e-28, tiny), sweep, converged, bytes, smraw, red);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(BG_NT, 1) k_svd_bgj_batch(const InstTask<T>* insts, const UpdRef* refs, int nref) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    for (int t = blockIdx.x; t < nref; t += gridDim.x) {
+        const UpdRef rf = refs[t];
+        const InstTask<T>& it = insts[rf.inst];
+        SvdParams pp = it.pp;
+        pp.bond = rf.op.bond;
+        svd_bgj_body<T>(it.mps, it.wk, pp, smraw);
+        __syncthreads();
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(BG_NT, 1) k_svd_bgj(MpsView<T> mps, SvdWork<T> wk, SvdParams pp) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    svd_bgj_body<T>(mps, wk, pp, smraw);
+}
+
+// Block-Gram Jacobi for one theta (insts == nullptr) or a batch, one CTA per theta.
+template <typename T>
+static void bgj_launch(const MpsView<T>* mps, const SvdWork<T>* wk, const SvdParams* pp, const InstTask<T>* insts,
+                       const UpdRef* refs, int nref, cudaStream_t s) {
+    size_t smem = BgShape<T>::smem;
+    const size_t sort_smem = 4096 * (sizeof(double) + sizeof(int));
+    if (smem < sort_smem) smem = sort_smem;
+    if (insts) {
+        auto fn = k_svd_bgj_batch<T>;
+        TQ_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int grid = num_sms();
+        if (grid > nref) grid = nref;
+        fn<<<grid, BG_NT, smem, s>>>(insts, refs, nref);
+    } else {
+        auto fn = k_svd_bgj<T>;
+        TQ_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        fn<<<1, BG_NT, smem, s>>>(*mps, *wk, *pp);
+    }
+    TQ_CHECK(cudaGetLastError());
+}
+
 template <typename T, int BW, int RPL>
 __global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd(MpsView<T> mps, SvdWork<T> wk, SvdParams pp) {
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -1641,14 +1989,19 @@ void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref,
     const int rows_cap = ((rows_ub + 7) & ~7) < 8 ? 8 : ((rows_ub + 7) & ~7);
     int rpl = 1;
     while (32 * rpl < rows_cap) rpl <<= 1;
-    if (rpl > 16) throw std::runtime_error("batched SVD supports at most 512 rows");
+    if (rpl > 16 && block_w != 0) throw std::runtime_error("the column-pair batched SVD supports at most 512 rows");
     int bw = block_w < 4 ? 4 : block_w;
     if (rpl == 16 && bw > 8) bw = 8;
     if (svd_begin) TQ_CHECK(cudaEventRecord(svd_begin, s));
     SvdParams rp{};
     rp.rows_cap = rows_cap;
     rp.cols_cap = rows_cap;  // every instance's theta is at most rows_ub x rows_ub
-    if (!res_dispatch<T>(nullptr, nullptr, rp, insts, refs, nref, s)) {
+    // small theta: resident Jacobi; large theta: block-Gram Jacobi unless an explicit block
+    // width asks for the column-pair kernel
+    if (res_dispatch<T>(nullptr, nullptr, rp, insts, refs, nref, s)) {
+    } else if (block_w == 0) {
+        bgj_launch<T>(nullptr, nullptr, nullptr, insts, refs, nref, s);
+    } else {
 #define TQ_RB(B, RP) \
     if (bw == B && rpl == RP) { svd_batch_bw<T, B, RP>(insts, refs, nref, rows_cap, s); } else
         TQ_RB(4, 1) TQ_RB(4, 2) TQ_RB(4, 4) TQ_RB(4, 8) TQ_RB(4, 16)

@@ -343,6 +343,16 @@ class Session:
         self._ck(self._L.tessera_qa_session_save(self._h, buf.ctypes.data, nb))
         return buf.tobytes()
 
+    def save_instance(self, index: int) -> bytes:
+        """Checkpoint of instance `index` of a batched session (tessera_qa_session_save_instance)."""
+        nb = self._L.tessera_qa_checkpoint_bytes(self.n_of(index), self.chi)
+        buf = np.zeros(nb, np.uint8)
+        self._ck(self._L.tessera_qa_session_save_instance(self._h, index, buf.ctypes.data, nb))
+        return buf.tobytes()
+
+    def n_of(self, index: int) -> int:
+        return int(self._Parr[index].n) if hasattr(self, "_Parr") else self.n
+
     def load(self, buf: bytes):
         a = np.frombuffer(buf, np.uint8).copy()
         self._ck(self._L.tessera_qa_session_load(self._h, a.ctypes.data, a.size))

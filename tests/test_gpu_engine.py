@@ -279,7 +279,7 @@ def test_resident_whole_anneal_matches_gate_slot_path():
     launches.  Both give the same anneals, also when instances outnumber the resident CTAs."""
     probs = [instances.dense_er(n, 300 + i, T=1.0, dt=0.1, chi=chi)
              for i, (n, chi) in enumerate([(16, 32), (12, 16), (9, 8), (14, 32), (5, 4), (11, 32)] * 3)]
-    probs += [instances.dense_er(4 + i % 3, 900 + i, T=0.3, dt=0.1, chi=4) for i in range(330)]
+    probs += [instances.dense_er(4 + i % 3, 900 + i, T=1.0, dt=0.1, chi=4) for i in range(330)]
     for prec, tol in (("c128", 1e-9), ("c64", 2e-4)):
         res = ffi.anneal_batch(probs, precision=prec)
         slot = ffi.anneal_batch(probs, precision=prec, jacobi_block=8)
@@ -289,3 +289,29 @@ def test_resident_whole_anneal_matches_gate_slot_path():
             assert a.expected_energy == pytest.approx(b.expected_energy, rel=tol, abs=tol), (p.name, prec)
             assert np.max(np.abs(a.entropy - b.entropy)) < 10 * tol, (p.name, prec)
             assert a.max_trunc == pytest.approx(b.max_trunc, rel=1e-2, abs=1e-12), (p.name, prec)
+
+
+@pytest.mark.parametrize("prec,tol", [("c128", 1e-10), ("c64", 1e-4)])
+def test_block_gram_batch_matches_column_pair_sessions(prec, tol):
+    """Large theta in a batch runs the block-Gram Jacobi (chi=64 complex128: a 128 x 128 theta,
+    256 KB, too big for the resident kernel); the same gate slots on single-instance sessions run
+    the cooperative column-pair kernel.  Random saturated MPS, updates with truncation: the
+    states agree to rounding and the discarded weights match."""
+    probs = [instances.chain_range(n=12, dmax=3, seed=s, T=1.0, dt=0.05, chi=64) for s in (4, 5)]
+    sb = ffi.Session.batch(probs, chi=64, precision=prec)
+    sb.randomize(11)
+    sb.run_gates(7, 0, 12)
+    rb = sb.sync()
+    assert rb.status == 0 and rb.two_site_updates == 24
+    for b, p in enumerate(probs):
+        s1 = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=64, precision=prec)
+        s1.randomize(11 + 7919 * b)
+        s1.run_gates(7, 0, 12)
+        r1 = s1.sync()
+        assert r1.status == 0
+        x = ffi.sites_to_dense(ffi.checkpoint_to_sites(s1.save())[1])
+        s1.close()
+        y = ffi.sites_to_dense(ffi.checkpoint_to_sites(sb.save_instance(b))[1])
+        assert 1 - fidelity(x, y) < tol, (prec, b)
+        assert np.vdot(y, y).real == pytest.approx(np.vdot(x, x).real, rel=tol)
+    sb.close()
