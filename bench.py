@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--profile-run", action="store_true",
                     help="one untimed step only (for ncu); prints no bench line")
     ap.add_argument("--profile-anneal", action="store_true",
-                    help="one batched anneal of 148 dense ER instances n=12, chi=32, T=1 (the small-bond resident "
+                    help="one batched anneal of 148 dense ER instances n=12, chi=32, T=0.3 (the small-bond resident "
                          "kernel, for ncu); prints no bench line")
     return ap.parse_args()
 
@@ -89,6 +89,26 @@ def max_over_ranks(ms: float, world: int, device: str = "cuda") -> float:
     t = torch.tensor([ms], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def fp64_peak_tflops() -> float:
+    """FP64 peak of this GPU as cuBLAS reaches it: best of 5 DGEMMs of 4096^3 (CUDA events)."""
+    import torch
+    a = torch.randn(4096, 4096, dtype=torch.float64, device="cuda")
+    b = torch.randn(4096, 4096, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    best = None
+    for _ in range(5):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    del a, b
+    return 2.0 * 4096 ** 3 / (best / 1e3) / 1e12
 
 
 def peaks():
@@ -286,12 +306,12 @@ def solves(args):
                       "best_candidate_solved": int((gaps.min(axis=1) <= 0.01).sum()),
                       "linear_solved": int((gaps[:, 0] <= 0.01).sum())},
             "workload": f"dense ER p=0.5, train n 8..12, held-out n 12..14, T={cfg.T}, dt={cfg.dt}, chi={cfg.chi}; "
-                        "reduced from config 5 (20k train n 8..20, 1024 eval n 24..48, chi=128, T=30)"}
+                        "reduced from the full learned-schedule study (20k train n 8..20, 1024 eval n 24..48, chi=128, T=30)"}
 
 
 def profile_anneal():
     from tessera_b200 import ffi, instances
-    probs = [instances.dense_er(12, 100 + i, T=1.0, dt=0.1, chi=32) for i in range(148)]
+    probs = [instances.dense_er(12, 100 + i, T=0.3, dt=0.1, chi=32) for i in range(148)]
     res = ffi.anneal_batch(probs, precision="c64", raise_on_status=False)
     print(f"profile anneal: {sum(r.two_site_updates for r in res)} updates, status "
           f"{sorted(set(r.status for r in res))}, {res[0].device_ms:.1f} ms")
@@ -378,6 +398,7 @@ def main():
     svd_n = r1.svd_launches - r0.svd_launches
     svd_ms = r1.svd_ms - r0.svd_ms
     svd_bytes = r1.svd_bytes - r0.svd_bytes
+    svd_flops = r1.svd_flops - r0.svd_flops
     launches = r1.kernel_launches - r0.kernel_launches
     sweeps = (r1.svd_sweeps - r0.svd_sweeps) / max(updates, 1)
     peak, peak_kind = peaks()
@@ -392,13 +413,30 @@ def main():
                 traffic = d.get("dram_bytes_per_launch")
         except Exception:
             traffic = None
-    kname = "k_svd_batch (one CTA per 512x512 theta)" if B > 1 else "k_svd (cooperative, 512x512 theta)"
+    if B == 1:
+        kname = "k_svd (cooperative column-pair Jacobi, 512x512 theta)"
+    elif args.jacobi_block == 32:
+        kname = "k_svd_bgj_batch (block-Gram Jacobi, one CTA per 512x512 theta)"
+    else:
+        kname = "k_svd_batch (column-pair Jacobi in blocks of 8, one CTA per 512x512 theta)"
     roofline = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak,
                 "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 "traffic": traffic, "avg_launch_ms": svd_ms / max(svd_n, 1),
                 "algorithmic_bytes_per_launch": svd_bytes / max(svd_n, 1), "avg_sweeps": sweeps,
                 "svd_share_of_step": svd_ms / ms if ms else None}
+
+    # the Jacobi arithmetic against the FP64 peak (the kernels compute in FP64: c128 data, FP64
+    # dot products and rotations)
+    try:
+        p64 = fp64_peak_tflops()
+    except Exception:
+        p64 = None
+    ach64 = svd_flops / (svd_ms / 1e3) / 1e12 if svd_ms else 0.0
+    compute_roofline = {"kernel": kname, "bound": "fp64", "achieved": ach64, "peak": p64, "unit": "TFLOP/s",
+                        "frac": ach64 / p64 if p64 else None,
+                        "peak_kind": "cuBLAS DGEMM 4096^3 measured in this run (best of 5)",
+                        "flops_per_launch": svd_flops / max(svd_n, 1)}
 
     # ---- e2e: host-buffer ABI call per step (values from pinned host memory, stats back) ----
     e2e = None
@@ -462,7 +500,8 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "c128" else "f32",
                 "data": "synthetic: seeded Ising instances (PCG64 seeds 2..) and seeded random MPS with every "
                         "bond at its cap",
-                "config": cfg, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "config": cfg, "roofline": roofline, "compute_roofline": compute_roofline, "cpu_baseline": cpu,
+                "e2e": e2e,
                 "gpu_launches": launches, "clocks": ck, "plain_single_instance": plain, "solves": sol,
                 "max_trunc_in_timed_steps": r1.max_trunc}
         print(json.dumps(line))

@@ -85,7 +85,9 @@ typedef struct tessera_qa_config {
     size_t chi;             /* bond-dimension cap */
     double jacobi_tol;      /* rotate a column pair when |w_p^H w_q| > tol |w_p||w_q|; 0 = default */
     int jacobi_max_sweeps;  /* 0 = default (60) */
-    int jacobi_block;       /* Jacobi column-block width (1,2,4,8,16); 0 = autotuned */
+    int jacobi_block;       /* 0 = chosen by size (resident Jacobi for small theta, else column pairs in blocks
+                               of 8); 1,2,4,8,16 = column-pair blocks of that width; 32 = block-Gram Jacobi
+                               (batches) */
     int device;             /* CUDA device ordinal; -1 = the calling thread's current device */
     size_t step_begin;      /* run schedule steps [step_begin, step_end) */
     size_t step_end;        /* 0 = problem.steps */
@@ -117,11 +119,12 @@ typedef struct tessera_qa_result {
     double min_cut_gap;     /* min over truncating updates of (s[keep-1] - s[keep]) / s[0]; 1 if none
                                truncated.  Near 0 the kept subspace is not unique (degenerate cut). */
     double svd_ms;          /* summed duration of the Jacobi-SVD launches (config.kernel_timing) */
-    double svd_bytes;       /* algorithmic bytes the Jacobi-SVD launches moved (see DESIGN) */
+    double svd_bytes;       /* bytes the Jacobi-SVD kernels read and wrote in global memory */
     long long svd_launches; /* Jacobi-SVD launches */
     long long svd_sweeps;   /* Jacobi sweeps summed over launches */
     long long kernel_launches; /* all engine kernel launches */
-    double reserved_d[2];
+    double svd_flops;       /* flops of the Jacobi arithmetic: dot products, rotations, Gram and apply GEMMs */
+    double reserved_d[1];
 } tessera_qa_result;
 
 /* Fills `cfg` with the legacy defaults: dt 0.1, zz_substeps 1, complex128, chi 32. */
@@ -133,7 +136,7 @@ TESSERA_QA_API void tessera_qa_config_init(tessera_qa_config* cfg);
 TESSERA_QA_API int tessera_qa_anneal_ex(const tessera_qa_problem* problem, const tessera_qa_config* config,
                          tessera_qa_result* result);
 
-/* Batched anneal of `count` independent instances (the north_star batching layer): each
+/* Batched anneal of `count` independent instances (the batching layer): each
  * instance runs exactly its own tessera_qa_anneal_ex (same gate order, keep rule, results),
  * but gate slot q of every instance goes into one launch of each batched kernel, with one
  * CTA per Jacobi SVD, so many updates run concurrently.  Instances may differ in n, edges,

@@ -46,7 +46,7 @@ class Result(C.Structure):
                 ("max_bond", C.c_int), ("reserved_i", C.c_int), ("device_ms", C.c_double),
                 ("min_cut_gap", C.c_double), ("svd_ms", C.c_double), ("svd_bytes", C.c_double),
                 ("svd_launches", C.c_longlong), ("svd_sweeps", C.c_longlong), ("kernel_launches", C.c_longlong),
-                ("reserved_d", C.c_double * 2)]
+                ("svd_flops", C.c_double), ("reserved_d", C.c_double * 1)]
 
 
 _lib = None

@@ -146,8 +146,8 @@ static Config validate_config(const tessera_qa_config* c) {
     if (c->chi > 1024) throw ArgError("chi > 1024 is not supported");
     if (c->precision != TESSERA_QA_C128 && c->precision != TESSERA_QA_C64) throw ArgError("unknown precision");
     if (c->jacobi_block && !(c->jacobi_block == 1 || c->jacobi_block == 2 || c->jacobi_block == 4 ||
-                             c->jacobi_block == 8 || c->jacobi_block == 16))
-        throw ArgError("jacobi_block must be 0, 1, 2, 4, 8 or 16");
+                             c->jacobi_block == 8 || c->jacobi_block == 16 || c->jacobi_block == 32))
+        throw ArgError("jacobi_block must be 0, 1, 2, 4, 8, 16 or 32 (32: block-Gram Jacobi, batches only)");
     if (c->jacobi_max_sweeps < 0 || c->jacobi_max_sweeps > 1000) throw ArgError("jacobi_max_sweeps out of range");
     C.dt = c->dt;
     C.ns = c->zz_substeps < 1 ? 1 : c->zz_substeps;
@@ -323,6 +323,7 @@ public:
         if (r) {
             r->svd_ms = svd_ms_;
             r->svd_bytes = st.svd_bytes;
+            r->svd_flops = st.svd_flops;
             r->svd_launches = svd_launches_;
             r->svd_sweeps = st.svd_sweeps;
             r->kernel_launches = launches_;
@@ -587,7 +588,7 @@ private:
     }
 
     int pick_block(int R, int N) const {
-        int b = C_.block;
+        int b = std::min(C_.block, 16);  // a single instance has no block-Gram path
         if (!b) {
             // default schedule: wide blocks for small matrices (few grid barriers), narrower
             // ones for large matrices (enough block pairs to fill the SMs)
@@ -826,7 +827,7 @@ public:
             q_max_ = std::max(q_max_, (int)eng_.back()->ops().size());
         }
         steps_ = steps;
-        block_ = C[0].block;  // 0: resident or block-Gram Jacobi by size; else column-pair blocks of this width
+        block_ = C[0].block;  // 0: by size (resident, else column pairs of width 8); 32: block-Gram
         rows_cap_ = std::max(8, (2 * cap_max_ + 7) & ~7);
         TQ_CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
         TQ_CK(cudaEventCreate(&e0_));
@@ -950,6 +951,7 @@ public:
             a.max_bond = std::max(a.max_bond, x.max_bond);
             a.min_cut_gap = std::min(a.min_cut_gap, x.min_cut_gap);
             a.svd_bytes += x.svd_bytes;
+            a.svd_flops += x.svd_flops;
             a.svd_sweeps += x.svd_sweeps;
         }
         r->two_site_updates = a.two_site_updates;
@@ -959,6 +961,7 @@ public:
         r->max_bond = a.max_bond;
         r->min_cut_gap = a.min_cut_gap;
         r->svd_bytes = a.svd_bytes;
+        r->svd_flops = a.svd_flops;
         r->svd_sweeps = a.svd_sweeps;
         r->svd_ms = svd_ms_;
         r->svd_launches = svd_launches_;
@@ -1378,6 +1381,7 @@ int tessera_qa_session_sync(tessera_qa_session* s, tessera_qa_result* result) {
             result->min_cut_gap = r.min_cut_gap;
             result->svd_ms = r.svd_ms;
             result->svd_bytes = r.svd_bytes;
+            result->svd_flops = r.svd_flops;
             result->svd_launches = r.svd_launches;
             result->svd_sweeps = r.svd_sweeps;
             result->kernel_launches = r.kernel_launches;

@@ -58,6 +58,7 @@ struct RunStats {
     double gap_deficit;     // max over truncating updates of 1 - (s[keep-1] - s[keep]) / s[0]
     double svd_bytes;       // algorithmic bytes moved by the Jacobi-SVD launches
     long long svd_sweeps;   // sweeps summed over launches
+    double svd_flops;       // FP64/FP32 flops of the Jacobi arithmetic (dot products, rotations, GEMMs)
 };
 
 // Per-update SVD workspace.

@@ -390,7 +390,7 @@ struct SvdShape {
 template <typename T>
 __device__ void svd_finish(const MpsView<T>& mps, const SvdWork<T>& wk, const SvdParams& pp, const int R, const int N,
                            const double keep_floor, const int sweep, const bool converged, const double bytes,
-                           unsigned char* smraw, double* red) {
+                           unsigned char* smraw, double* red, const double flops = 0.0) {
     const int tid = threadIdx.x;
     const int NT = blockDim.x, NW = NT >> 5;
     int P2 = 1;
@@ -471,6 +471,7 @@ __device__ void svd_finish(const MpsView<T>& mps, const SvdWork<T>& wk, const Sv
         if (sweep > st->max_sweeps) st->max_sweeps = sweep;
         st->svd_sweeps += sweep;
         st->svd_bytes += bytes;
+        st->svd_flops += flops;
         if (keep > st->max_bond) st->max_bond = keep;
         st->updates += 1;
         mps.dims[pp.bond + 1] = keep;
@@ -693,8 +694,12 @@ __device__ __forceinline__ void svd_body(const MpsView<T>& mps, const SvdWork<T>
     }
     if (!cta_sync(wk.bar, status, nblk)) return;
     if (cta != 0) return;
+    // pairs evaluated (16 flops per row: four FP64 dot products) and rotated (32 per row)
+    double rots = 0.0;
+    for (int e = 0; e < sweep && e < pp.max_sweeps; ++e) rots += (double)(*(volatile int*)&wk.counters[e]);
+    const double flops = (double)sweep * 0.5 * N * (N - 1) * R * 16.0 + rots * R * 32.0;
     svd_finish<T>(mps, wk, pp, R, N, keep_floor, sweep, converged,
-                  ((double)sweep * (P - 1) * 2.0 + 2.0) * (double)R * N * sizeof(V), smraw, red);
+                  ((double)sweep * (P - 1) * 2.0 + 2.0) * (double)R * N * sizeof(V), smraw, red, flops);
 }
 
 // ------------------------------------------------------------------------------------
@@ -714,7 +719,8 @@ constexpr int RES_RPL = 8;  // register rows per lane; R <= LPP * RES_RPL
 
 template <typename T, int LPP>
 __device__ void jacobi_core(cplx_t<T>* col, const int rc, const int R, const int N, const double tol,
-                            const double tiny, const int max_sweeps, int* s_rot, int& sweeps, bool& converged) {
+                            const double tiny, const int max_sweeps, int* s_rot, int& sweeps, bool& converged,
+                            double& rotations) {
     using V = cplx_t<T>;
     constexpr int PPW = 32 / LPP;
     constexpr int RPL = RES_RPL;
@@ -730,6 +736,7 @@ __device__ void jacobi_core(cplx_t<T>* col, const int rc, const int R, const int
     __syncthreads();
     int sweep = 0;
     converged = false;
+    rotations = 0.0;
     for (; sweep < max_sweeps; ++sweep) {
         int rot = 0;
         for (int r = 0; r < Nc - 1; ++r) {
@@ -789,6 +796,7 @@ __device__ void jacobi_core(cplx_t<T>* col, const int rc, const int R, const int
         __syncthreads();
         const int done = s_rot[sweep & 1];
         if (tid == 0) s_rot[(sweep + 1) & 1] = 0;
+        rotations += done;
         if (done == 0) {
             converged = true;
             ++sweep;
@@ -875,10 +883,12 @@ __device__ void svd_resident_body(const MpsView<T>& mps, const SvdWork<T>& wk, c
     const double tiny = noise_tiny(pp.tiny, R, block_fro2<T>(col, rc, R, N, red), sizeof(T) == 4);
     int sweep = 0;
     bool converged = false;
-    jacobi_core<T, LPP>(col, rc, R, N, pp.tol, tiny, pp.max_sweeps, s_rot, sweep, converged);
+    double rots = 0.0;
+    jacobi_core<T, LPP>(col, rc, R, N, pp.tol, tiny, pp.max_sweeps, s_rot, sweep, converged, rots);
     resident_norms<T>(col, rc, R, N, wk.W, ld, wk.sig2);
+    const double flops = (double)sweep * 0.5 * N * (N - 1) * R * 16.0 + rots * R * 32.0;
     svd_finish<T>(mps, wk, pp, R, N, fmax(1e-28, tiny), sweep, converged, 2.0 * (double)R * N * sizeof(V), smraw,
-                  red);
+                  red, flops);
 }
 
 template <typename T, int LPP>
@@ -967,13 +977,15 @@ __device__ void resident_update(const MpsView<T>& mps, const ScheduleView& sch, 
     const double tiny = noise_tiny(pp0.tiny, R, block_fro2<T>(col, rc, R, N, red), sizeof(T) == 4);
     int sweep = 0;
     bool converged = false;
-    jacobi_core<T, LPP>(col, rc, R, N, pp0.tol, tiny, pp0.max_sweeps, s_rot, sweep, converged);
+    double rots = 0.0;
+    jacobi_core<T, LPP>(col, rc, R, N, pp0.tol, tiny, pp0.max_sweeps, s_rot, sweep, converged, rots);
     resident_norms<T>(col, rc, R, N, nullptr, ld, wk.sig2);
     SvdParams pp = pp0;
     pp.bond = i;
     // global traffic of the update: A and C read, theta written and read back, A' and C' written
     const double bytes = (double)sizeof(V) * (2.0 * dl * mid + 2.0 * mid * dr + 3.0 * R * N);
-    svd_finish<T>(mps, wk, pp, R, N, fmax(1e-28, tiny), sweep, converged, bytes, sortbuf, red);
+    const double flops = (double)sweep * 0.5 * N * (N - 1) * R * 16.0 + rots * R * 32.0;
+    svd_finish<T>(mps, wk, pp, R, N, fmax(1e-28, tiny), sweep, converged, bytes, sortbuf, red, flops);
     __syncthreads();
     const int keep = mps.dims[i + 1];
     // A' (a, s1, k) = W[(2a+s1), perm k] / sigma_k
@@ -1230,7 +1242,7 @@ __device__ __forceinline__ bool bg_wait(uint64_t* bar, unsigned& ph, int* s_ok) 
 template <typename T>
 __device__ bool bg_pair(const SvdWork<T>& wk, int R, int N, int I, int J, double tol, double tiny, double2* G,
                         double2* Vm, cplx_t<T>* ch0, cplx_t<T>* ch1, uint64_t* bars, unsigned* phase, BgRot* prm,
-                        int* s_rot, double* bytes) {
+                        int* s_rot, double* bytes, double* flops) {
     using V = cplx_t<T>;
     constexpr int CS = BgShape<T>::CS;
     const int tid = threadIdx.x;
@@ -1283,6 +1295,7 @@ __device__ bool bg_pair(const SvdWork<T>& wk, int R, int N, int I, int J, double
     if (tid == 0) s_rot[1] = 0;
     __syncthreads();
     *bytes += (double)nvalid * R * sizeof(V);
+    *flops += 8.0 * nvalid * nvalid * R;  // Gram: one complex multiply-add per entry and row
     // ---- 2. one cyclic two-sided Jacobi sweep on G, V accumulated ----
     for (int rd = 0; rd < BG_W - 1; ++rd) {
         if (tid < BG_W / 2) {
@@ -1329,6 +1342,9 @@ __device__ bool bg_pair(const SvdWork<T>& wk, int R, int N, int I, int J, double
         __syncthreads();
     }
     const int nrot = s_rot[1];
+    // a two-sided rotation updates two columns of G and V and two rows of G: 3 x 64 x 2 complex
+    // entries at 16 flops each
+    *flops += (double)nrot * 3.0 * BG_W * 2.0 * 16.0;
     if (nrot == 0) return true;
     if (tid == 0) s_rot[0] += nrot;
     // ---- 3. Wp <- Wp V: thread (tr, tc) owns chunk row tr, columns tc + 8m ----
@@ -1365,6 +1381,7 @@ __device__ bool bg_pair(const SvdWork<T>& wk, int R, int N, int I, int J, double
     fence_proxy_async_global();
     __syncthreads();
     *bytes += 2.0 * (double)nvalid * R * sizeof(V);
+    *flops += 8.0 * BG_W * nvalid * R;  // apply: 64 complex multiply-adds per output element
     return true;
 }
 
@@ -1406,6 +1423,7 @@ __device__ void svd_bgj_body(const MpsView<T>& mps, const SvdWork<T>& wk, const 
     const int nb = (N + BG_B - 1) / BG_B;
     const int P = nb + (nb & 1);
     double bytes = (double)R * N * sizeof(V);
+    double flops = 0.0;
     int sweep = 0;
     bool converged = false;
     for (; sweep < pp.max_sweeps; ++sweep) {
@@ -1415,7 +1433,8 @@ __device__ void svd_bgj_body(const MpsView<T>& mps, const SvdWork<T>& wk, const 
             for (int pr = 0; pr < P / 2; ++pr) {
                 int I, J;
                 tournament(P, r, pr, I, J);
-                if (!bg_pair<T>(wk, R, N, I, J, pp.tol, tiny, G, Vm, ch0, ch1, bars, phase, prm, s_rot, &bytes)) {
+                if (!bg_pair<T>(wk, R, N, I, J, pp.tol, tiny, G, Vm, ch0, ch1, bars, phase, prm, s_rot, &bytes,
+                                &flops)) {
                     // every thread leaves here together; wait (bounded) for the copies still in
                     // flight so that none lands in shared memory after the CTA has moved on
                     if (tid == 0) {
@@ -1446,7 +1465,7 @@ __device__ void svd_bgj_body(const MpsView<T>& mps, const SvdWork<T>& wk, const 
     }
     __syncthreads();
     bytes += (double)R * N * sizeof(V);
-    svd_finish<T>(mps, wk, pp, R, N, fmax(1e-28, tiny), sweep, converged, bytes, smraw, red);
+    svd_finish<T>(mps, wk, pp, R, N, fmax(1e-28, tiny), sweep, converged, bytes, smraw, red, flops);
 }
 
 template <typename T>
@@ -1989,17 +2008,18 @@ void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref,
     const int rows_cap = ((rows_ub + 7) & ~7) < 8 ? 8 : ((rows_ub + 7) & ~7);
     int rpl = 1;
     while (32 * rpl < rows_cap) rpl <<= 1;
-    if (rpl > 16 && block_w != 0) throw std::runtime_error("the column-pair batched SVD supports at most 512 rows");
+    if (rpl > 16 && block_w != BG_B) throw std::runtime_error("the column-pair batched SVD supports at most 512 rows");
     int bw = block_w < 4 ? 4 : block_w;
     if (rpl == 16 && bw > 8) bw = 8;
     if (svd_begin) TQ_CHECK(cudaEventRecord(svd_begin, s));
     SvdParams rp{};
     rp.rows_cap = rows_cap;
     rp.cols_cap = rows_cap;  // every instance's theta is at most rows_ub x rows_ub
-    // small theta: resident Jacobi; large theta: block-Gram Jacobi unless an explicit block
-    // width asks for the column-pair kernel
+    // small theta: resident Jacobi; large theta: the column-pair kernel (block width 8, or the
+    // one asked for), or the block-Gram kernel when block width 32 is asked for
+    if (block_w == 0) bw = 8;
     if (res_dispatch<T>(nullptr, nullptr, rp, insts, refs, nref, s)) {
-    } else if (block_w == 0) {
+    } else if (block_w == BG_B) {
         bgj_launch<T>(nullptr, nullptr, nullptr, insts, refs, nref, s);
     } else {
 #define TQ_RB(B, RP) \

