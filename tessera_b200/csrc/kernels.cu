@@ -1514,6 +1514,225 @@ __global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd(MpsView<T> mps
     svd_body<T, BW, RPL>(mps, wk, pp, blockIdx.x, gridDim.x, smraw);
 }
 
+// ------------------------------------------------------------------------------------
+// K2b: the batched column-pair Jacobi (one CTA per theta), block-row-cyclic.  With one CTA
+// per theta the block pairs need not be disjoint within a round, so the sweep runs them in
+// row-cyclic order: for each block I, first its BW(BW-1)/2 inner pairs (staged in shared
+// memory), then block I stays in registers (warp w holds column w, RPL rows per lane) while
+// the blocks J > I stream past it, two shared-memory buffers deep: the 1-D TMA bulk copy of
+// block J+1 runs under the BW cross rounds of block J, and only J is written back after
+// them.  Per sweep the columns move (nb + nb(nb-1)/2) times in each direction instead of
+// 2 (P-1) P/2 times, and no copy waits in the open.  Every pair is visited once per sweep
+// (a cyclic ordering), with the rotation of jacobi_rotation.
+// ------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void rc_stage(cplx_t<T>* dst, const cplx_t<T>* W, int ld, int rc, int R, int N, int blk,
+                                         int BW, uint64_t* bar) {
+    using V = cplx_t<T>;
+    unsigned nv = 0;
+    for (int c = 0; c < BW; ++c) nv += blk * BW + c < N;
+    const unsigned bytes = (unsigned)(R * sizeof(V));
+    fence_proxy_async_shared();
+    mbar_expect_tx(bar, nv * bytes);
+    for (int c = 0; c < BW; ++c)
+        if (blk * BW + c < N) tma_load_1d(dst + c * rc, W + (long long)(blk * BW + c) * ld, bytes, bar);
+}
+
+template <typename T, int BW, int RPL>
+__device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const SvdParams& pp, unsigned char* smraw) {
+    using V = cplx_t<T>;
+    constexpr int NT = 32 * BW;
+    constexpr int NW = BW;
+    constexpr int G2 = 2 * NT / BW;  // threads per pair of the inner rounds (BW/2 pairs)
+    static_assert(RPL > 0, "register-resident rows");
+    __shared__ double red[4 * NW];
+    __shared__ int s_rot;
+    __shared__ int s_ok;
+    __shared__ __align__(8) uint64_t bars[3];  // [0] block I, [1], [2] the two J buffers
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int R = pp.R > 0 ? pp.R : 2 * mps.dims[pp.bond];
+    const int N = pp.N > 0 ? pp.N : 2 * mps.dims[pp.bond + 2];
+    const int rc = pp.rows_cap;
+    const int ld = wk.ld;
+    V* W = wk.W;
+    int* status = &wk.stats->status;
+    if (R > rc || R > 32 * RPL) {  // host sizing bug guard
+        if (tid == 0) atomicOr(status, ST_BAD_DIMS);
+        return;
+    }
+    V* ci = reinterpret_cast<V*>(smraw);  // [BW][rc]
+    V* cj[2] = {ci + BW * rc, ci + 2 * BW * rc};
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init(&bars[2], 1);
+    }
+    unsigned ph[3] = {0u, 0u, 0u};
+    // one CTA-wide outcome per copy wait (thread 0 waits, the others re-check the phase)
+    auto wait = [&](int k) -> bool {
+        if (tid == 0) s_ok = mbar_wait(&bars[k], ph[k], 1000000000ull) ? 1 : 0;
+        __syncthreads();
+        const bool ok = s_ok != 0;
+        if (ok && tid != 0) mbar_wait(&bars[k], ph[k], 1000000000ull);
+        if (ok) ph[k] ^= 1u;
+        return ok;
+    };
+    // ||W||_F^2 for the noise floor
+    double part = 0.0;
+    for (int j = warp; j < N; j += NW) {
+        const V* w = W + (long long)j * ld;
+        double sj = 0.0;
+        for (int row = lane; row < R; row += 32) sj += (double)w[row].x * w[row].x + (double)w[row].y * w[row].y;
+        part += warp_sum(sj);
+    }
+    if (lane == 0) red[warp] = part;
+    __syncthreads();
+    double fro2 = 0.0;
+    for (int w = 0; w < NW; ++w) fro2 += red[w];
+    const double tiny = noise_tiny(pp.tiny, R, fro2, sizeof(T) == 4);
+    __syncthreads();
+    const int nb = (N + BW - 1) / BW;
+    double rots_total = 0.0;
+    int sweep = 0;
+    bool converged = false;
+    bool fail = false;
+    for (; sweep < pp.max_sweeps && !fail; ++sweep) {
+        if (tid == 0) s_rot = 0;
+        __syncthreads();
+        int rot = 0;
+        for (int I = 0; I < nb && !fail; ++I) {
+            if (tid == 0) rc_stage<T>(ci, W, ld, rc, R, N, I, BW, &bars[0]);
+            if (!wait(0)) { fail = true; break; }
+            // inner pairs of block I: circle method, BW/2 pairs per round, G2 threads each
+            {
+                const int ip = tid / G2;
+                for (int t = 0; t < BW - 1; ++t) {
+                    int x, y;
+                    if (ip == 0) { x = BW - 1; y = t; }
+                    else { x = (t + ip) % (BW - 1); y = (t - ip + (BW - 1)) % (BW - 1); }
+                    const bool ok = (I * BW + x < N) && (I * BW + y < N);
+                    const int r1 = rotate_pair<T, G2>(ci + x * rc, ci + y * rc, ok, R, pp.tol, tiny, red, tid);
+                    if (r1 && (tid % G2) == 0) ++rot;
+                    __syncthreads();
+                }
+            }
+            const bool vi = I * BW + warp < N;
+            V xi[RPL];
+#pragma unroll
+            for (int k = 0; k < RPL; ++k) {
+                const int row = lane + 32 * k;
+                xi[k] = row < R ? ci[warp * rc + row] : czero<V>();
+            }
+            __syncthreads();  // ci free for the next block I
+            if (I + 1 < nb && tid == 0) rc_stage<T>(cj[0], W, ld, rc, R, N, I + 1, BW, &bars[1]);
+            for (int J = I + 1; J < nb; ++J) {
+                const int b = (J - I - 1) & 1;
+                if (J + 1 < nb && tid == 0) rc_stage<T>(cj[b ^ 1], W, ld, rc, R, N, J + 1, BW, &bars[1 + (b ^ 1)]);
+                if (!wait(1 + b)) { fail = true; break; }
+                V* cb = cj[b];
+                for (int t = 0; t < BW; ++t) {
+                    const int q = (warp + t) % BW;
+                    const bool ok = vi && (J * BW + q < N);
+                    V* cq = cb + q * rc;
+                    V yj[RPL];
+#pragma unroll
+                    for (int k = 0; k < RPL; ++k) {
+                        const int row = lane + 32 * k;
+                        yj[k] = (ok && row < R) ? cq[row] : czero<V>();
+                    }
+                    double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+#pragma unroll
+                    for (int k = 0; k < RPL; ++k) {
+                        const V x = xi[k], y = yj[k];
+                        v0 += (double)x.x * x.x + (double)x.y * x.y;
+                        v1 += (double)y.x * y.x + (double)y.y * y.y;
+                        v2 += (double)x.x * y.x + (double)x.y * y.y;
+                        v3 += (double)x.x * y.y - (double)x.y * y.x;
+                    }
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        v0 += __shfl_xor_sync(0xffffffffu, v0, o);
+                        v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+                        v2 += __shfl_xor_sync(0xffffffffu, v2, o);
+                        v3 += __shfl_xor_sync(0xffffffffu, v3, o);
+                    }
+                    T c, sn, er, ei;
+                    if (ok && jacobi_rotation<T>(v0, v1, v2, v3, pp.tol, tiny, c, sn, er, ei)) {
+#pragma unroll
+                        for (int k = 0; k < RPL; ++k) {
+                            const V x = xi[k], y = yj[k];
+                            const T ey_re = er * y.x + ei * y.y, ey_im = er * y.y - ei * y.x;
+                            const T ex_re = er * x.x - ei * x.y, ex_im = er * x.y + ei * x.x;
+                            xi[k] = mk<V>(c * x.x - sn * ey_re, c * x.y - sn * ey_im);
+                            yj[k] = mk<V>(sn * ex_re + c * y.x, sn * ex_im + c * y.y);
+                        }
+#pragma unroll
+                        for (int k = 0; k < RPL; ++k) {
+                            const int row = lane + 32 * k;
+                            if (row < R) cq[row] = yj[k];
+                        }
+                        if (lane == 0) ++rot;
+                    }
+                    __syncthreads();
+                }
+                // block J back to global memory; later bulk copies read it
+                for (int c = warp; c < BW; c += NW) {
+                    if (J * BW + c >= N) continue;
+                    V* dst = W + (long long)(J * BW + c) * ld;
+                    const V* src = cb + c * rc;
+                    for (int row = lane; row < R; row += 32) dst[row] = src[row];
+                }
+                fence_proxy_async_global();
+                __syncthreads();
+            }
+            if (fail) break;
+            if (vi) {
+                V* dst = W + (long long)(I * BW + warp) * ld;
+#pragma unroll
+                for (int k = 0; k < RPL; ++k) {
+                    const int row = lane + 32 * k;
+                    if (row < R) dst[row] = xi[k];
+                }
+            }
+            fence_proxy_async_global();
+            __syncthreads();
+        }
+        if (fail) break;
+        if (rot) atomicAdd(&s_rot, rot);
+        __syncthreads();
+        const int done = s_rot;
+        __syncthreads();
+        rots_total += done;
+        if (done == 0) {
+            converged = true;
+            ++sweep;
+            break;
+        }
+    }
+    if (fail) {
+        // every thread leaves together; wait (bounded) for copies still in flight
+        if (tid == 0) {
+            atomicOr(status, ST_BARRIER_TIMEOUT);
+            for (int k = 0; k < 3; ++k) mbar_wait(&bars[k], ph[k], 1000000000ull);
+        }
+        __syncthreads();
+        return;
+    }
+    // column norms -> sig2 (FP64)
+    for (int j = warp; j < N; j += NW) {
+        const V* w = W + (long long)j * ld;
+        double sj = 0.0;
+        for (int row = lane; row < R; row += 32) sj += (double)w[row].x * w[row].x + (double)w[row].y * w[row].y;
+        sj = warp_sum(sj);
+        if (lane == 0) wk.sig2[j] = sj;
+    }
+    __syncthreads();
+    const double moves = (double)sweep * ((double)nb + 0.5 * nb * (nb - 1)) * 2.0 + 2.0;
+    const double flops = (double)sweep * 0.5 * N * (N - 1) * R * 16.0 + rots_total * R * 32.0;
+    svd_finish<T>(mps, wk, pp, R, N, fmax(1e-28, tiny), sweep, converged, moves * (double)BW * R * sizeof(V), smraw,
+                  red, flops);
+}
+
 // Batched: each CTA takes whole SVD tasks (one theta each) in turn; no inter-CTA waits.
 template <typename T, int BW, int RPL>
 __global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd_batch(const InstTask<T>* insts, const UpdRef* refs,
@@ -1524,7 +1743,8 @@ __global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd_batch(const In
         const InstTask<T>& it = insts[rf.inst];
         SvdParams pp = it.pp;
         pp.bond = rf.op.bond;
-        svd_body<T, BW, RPL>(it.mps, it.wk, pp, 0, 1, smraw);
+        if constexpr (RPL > 0) svd_body_rc<T, BW, RPL>(it.mps, it.wk, pp, smraw);
+        else svd_body<T, BW, RPL>(it.mps, it.wk, pp, 0, 1, smraw);
         __syncthreads();
     }
 }
@@ -1984,7 +2204,8 @@ template <typename T, int BW, int RPL>
 static void svd_batch_bw(const InstTask<T>* insts, const UpdRef* refs, int nref, int rows_cap, cudaStream_t s) {
     using V = cplx_t<T>;
     constexpr int NT = SvdShape<BW, RPL>::NT;
-    size_t smem = sizeof(V) * 2 * BW * (size_t)rows_cap;
+    // block-row-cyclic (RPL > 0): block I plus two J buffers; else one staged block pair
+    size_t smem = sizeof(V) * (RPL > 0 ? 3 : 2) * BW * (size_t)rows_cap;
     const size_t sort_smem = 4096 * (sizeof(double) + sizeof(int));
     if (smem < sort_smem) smem = sort_smem;
     auto fn = k_svd_batch<T, BW, RPL>;

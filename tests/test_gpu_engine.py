@@ -283,7 +283,9 @@ def test_resident_whole_anneal_matches_gate_slot_path():
     probs = [instances.dense_er(n, 300 + i, T=1.0, dt=0.1, chi=chi)
              for i, (n, chi) in enumerate([(10, 32), (8, 16), (9, 16), (11, 32), (5, 4), (7, 8)] * 3)]
     probs += [instances.dense_er(4 + i % 3, 900 + i, T=1.0, dt=0.1, chi=8) for i in range(330)]
-    for prec, tol in (("c128", 1e-9), ("c64", 2e-4)):
+    # complex64 rounds differently on the two paths; over ~1000 unitary updates its own error
+    # against complex128 reaches ~1e-4 relative on these dense instances
+    for prec, tol in (("c128", 1e-9), ("c64", 2e-3)):
         res = ffi.anneal_batch(probs, precision=prec)
         slot = ffi.anneal_batch(probs, precision=prec, jacobi_block=8)
         for p, a, b in zip(probs, res, slot):
@@ -291,17 +293,24 @@ def test_resident_whole_anneal_matches_gate_slot_path():
             assert a.two_site_updates == b.two_site_updates, p.name
             assert a.expected_energy == pytest.approx(b.expected_energy, rel=tol, abs=tol), (p.name, prec)
             assert np.max(np.abs(a.entropy - b.entropy)) < 10 * tol, (p.name, prec)
+            if prec == "c64":
+                ref = ffi.anneal(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=p.chi, precision="c128") \
+                    if p.n >= 9 else None
+                if ref is not None:
+                    assert a.expected_energy == pytest.approx(ref.expected_energy, rel=tol), p.name
             assert a.max_trunc < 1e-9 and b.max_trunc < 1e-9, (p.name, prec)
 
 
+@pytest.mark.parametrize("block", [0, 32])
 @pytest.mark.parametrize("prec,n,chi,q0,tol", [("c128", 12, 64, 36, 1e-10), ("c64", 16, 128, 54, 1e-4)])
-def test_block_gram_batch_matches_column_pair_sessions(prec, n, chi, q0, tol):
-    """Large theta in a batch with jacobi_block = 32 runs the block-Gram Jacobi (128 x 128
-    complex128 or 256 x 256 complex64 theta: too big for the resident kernel); the same gate slots
-    on single-instance sessions run the cooperative column-pair kernel.  Random saturated MPS, interior bonds,
-    truncating updates: the states agree to rounding and the runs are clean."""
+def test_large_theta_batch_matches_cooperative_sessions(prec, n, chi, q0, tol, block):
+    """Large theta in a batch (128 x 128 complex128 or 256 x 256 complex64: too big for the
+    resident kernel) runs the block-row-cyclic column-pair Jacobi (jacobi_block 0) or the
+    block-Gram Jacobi (32); the same gate slots on single-instance sessions run the cooperative
+    column-pair kernel.  Random saturated MPS, interior bonds, truncating updates: the states
+    agree to rounding and the runs are clean."""
     probs = [instances.chain_range(n=n, dmax=3, seed=s, T=1.0, dt=0.05, chi=chi) for s in (4, 5)]
-    sb = ffi.Session.batch(probs, chi=chi, precision=prec, jacobi_block=32)
+    sb = ffi.Session.batch(probs, chi=chi, precision=prec, jacobi_block=block)
     sb.randomize(11)
     sb.run_gates(7, q0, q0 + 12)
     rb = sb.sync()
