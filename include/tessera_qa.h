@@ -94,7 +94,9 @@ typedef struct tessera_qa_config {
     const void* initial_mps;/* NULL = |+>^n; else a checkpoint written by a previous call */
     int skip_observables;   /* 1 = skip the final <Z>, <ZZ>, readout and prob (checkpoint runs) */
     int kernel_timing;      /* 1 = time every Jacobi-SVD launch with CUDA events (result.svd_ms) */
-    int reserved[6];
+    int theta_tensor_cores; /* complex64 only: 1 = bond contraction on the tcgen05 tensor cores in split-TF32
+                               (three TF32 passes, FP32 accumulators); 0 = CUDA-core FP32 */
+    int reserved[5];
 } tessera_qa_config;
 
 typedef struct tessera_qa_result {

@@ -35,7 +35,7 @@ class Config(C.Structure):
                 ("jacobi_tol", C.c_double), ("jacobi_max_sweeps", C.c_int), ("jacobi_block", C.c_int),
                 ("device", C.c_int), ("step_begin", C.c_size_t), ("step_end", C.c_size_t),
                 ("initial_mps", C.c_void_p), ("skip_observables", C.c_int), ("kernel_timing", C.c_int),
-                ("reserved", C.c_int * 6)]
+                ("theta_tensor_cores", C.c_int), ("reserved", C.c_int * 5)]
 
 
 class Result(C.Structure):

@@ -136,6 +136,7 @@ struct Config {
     int device = -1;
     int min_ld = 0;  // workspace rows/cols at least this (standalone SVD)
     int timing = 0;  // time each SVD launch with CUDA events
+    int theta_tc = 0;  // complex64: bond contraction on tcgen05 tensor cores (split-TF32)
 };
 
 static Config validate_config(const tessera_qa_config* c) {
@@ -158,6 +159,9 @@ static Config validate_config(const tessera_qa_config* c) {
     C.block = c->jacobi_block;
     C.device = c->device;
     C.timing = c->kernel_timing;
+    C.theta_tc = c->theta_tensor_cores;
+    if (C.theta_tc && c->precision != TESSERA_QA_C64)
+        throw ArgError("theta_tensor_cores needs complex64 precision");
     return C;
 }
 
@@ -250,7 +254,7 @@ public:
         // small bonds (theta fits one CTA's shared memory): the whole run is one launch of the
         // resident anneal kernel, the same code a batch runs for each of its instances; the
         // per-update path stays for large bonds, explicit Jacobi block widths and SVD timing
-        if (k1 > k0 && C_.block == 0 && !C_.timing && n_ >= 1) {
+        if (k1 > k0 && C_.block == 0 && !C_.timing && !C_.theta_tc && n_ >= 1) {
             const int rc = std::max(8, (2 * cap_ + 7) & ~7);
             ensure_resident(rc);
             if (launch_anneal_resident<T>(res_inst_, res_ops_, res_off_, res_order_, 1, k0, k1, res_work_, rc,
@@ -750,7 +754,14 @@ private:
         const int i = op.bond;
         const int dl = ub_[i], dr = ub_[i + 2];
         const int keep_ub = std::min(C_.chi, std::min(2 * dl, 2 * dr));
-        launch_theta<T>(M, sch, op, nullptr, work(), dl, dr, stream_);
+        bool tc_done = false;
+        if constexpr (sizeof(T) == 4) {
+            if (C_.theta_tc && theta_tc_supported(op)) {
+                launch_theta_tc(M, sch, op, work(), dl, dr, stream_);
+                tc_done = true;
+            }
+        }
+        if (!tc_done) launch_theta<T>(M, sch, op, nullptr, work(), dl, dr, stream_);
         cudaEvent_t a = nullptr, b = nullptr;
         if (C_.timing) {
             a = event();
@@ -879,7 +890,8 @@ public:
             TQ_CK(cudaMemcpy(ops_all_, ops_all.data(), sizeof(GateOp) * ops_all.size(), cudaMemcpyHostToDevice));
         TQ_CK(cudaMemcpy(op_off_, op_off.data(), sizeof(int) * (B + 1), cudaMemcpyHostToDevice));
         TQ_CK(cudaMemcpy(order_, order.data(), sizeof(int) * B, cudaMemcpyHostToDevice));
-        resident_ = C[0].block == 0;
+        resident_ = C[0].block == 0 && !C[0].theta_tc;
+        theta_tc_ = C[0].theta_tc != 0;
         for (auto& e : eng_) TQ_CK(cudaStreamSynchronize(e->own_stream()));
     }
     ~BatchEngine() override {
@@ -1010,7 +1022,8 @@ private:
             a = event();
             b = event();
         }
-        launch_update_batch<T>(insts_, refs_ + refs_off_[q], nref, cap_max_, 2 * cap_max_, block_, st_, a, b);
+        launch_update_batch<T>(insts_, refs_ + refs_off_[q], nref, cap_max_, 2 * cap_max_, block_, st_, a, b,
+                               theta_tc_);
         if (timing_) timed_.push_back({a, b});
         launches_ += 4;
         ++svd_launches_;
@@ -1043,6 +1056,7 @@ private:
     GateOp* ops_all_ = nullptr;
     int *op_off_ = nullptr, *order_ = nullptr, *work_ = nullptr;
     bool resident_ = true;
+    bool theta_tc_ = false;
     std::vector<size_t> refs_off_;
     int cap_max_ = 1, n_max_ = 1, q_max_ = 0, steps_ = 0, block_ = 8, rows_cap_ = 8;
     double ms_ = 0.0;

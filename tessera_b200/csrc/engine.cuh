@@ -160,7 +160,7 @@ void launch_single_site_batch(const InstTask<T>* insts, int ninst, int n_max, in
 template <typename T>
 void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref, int d_ub, int rows_ub,
                          int block_w, cudaStream_t s, cudaEvent_t svd_begin = nullptr,
-                         cudaEvent_t svd_end = nullptr);
+                         cudaEvent_t svd_end = nullptr, bool theta_tc = false);
 template <typename T>
 void launch_entropy_batch(const InstTask<T>* insts, int ninst, cudaStream_t s);
 // Whole anneal of every instance, one CTA per instance at a time (small bonds only); false
@@ -168,6 +168,11 @@ void launch_entropy_batch(const InstTask<T>* insts, int ninst, cudaStream_t s);
 template <typename T>
 bool launch_anneal_resident(const InstTask<T>* insts, const GateOp* ops, const int* op_off, const int* order,
                             int ninst, int k0, int k1, int* work, int rows_cap, cudaStream_t s);
+// complex64 bond contraction on tcgen05 tensor cores, split-TF32 (theta_tc.cu)
+bool theta_tc_supported(const GateOp& op);
+void launch_theta_tc(const MpsView<float>& mps, const ScheduleView& sch, GateOp op, SvdWork<float> wk, int dl_ub,
+                     int dr_ub, cudaStream_t s);
+void launch_theta_tc_batch(const InstTask<float>* insts, const UpdRef* refs, int nref, int d_ub, cudaStream_t s);
 template <typename T>
 void launch_init_plus(const MpsView<T>& mps, cudaStream_t s);
 

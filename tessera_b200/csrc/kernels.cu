@@ -2221,10 +2221,19 @@ static void svd_batch_bw(const InstTask<T>* insts, const UpdRef* refs, int nref,
 
 template <typename T>
 void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref, int d_ub, int rows_ub,
-                         int block_w, cudaStream_t s, cudaEvent_t svd_begin, cudaEvent_t svd_end) {
+                         int block_w, cudaStream_t s, cudaEvent_t svd_begin, cudaEvent_t svd_end, bool theta_tc) {
     if (nref <= 0) return;
-    const int tiles = (d_ub + 31) / 32;
-    k_theta_batch<T><<<dim3(tiles, tiles, nref), 256, 0, s>>>(insts, refs);
+    if constexpr (sizeof(T) == 4) {
+        if (theta_tc) {
+            launch_theta_tc_batch(reinterpret_cast<const InstTask<float>*>(insts), refs, nref, d_ub, s);
+        } else {
+            const int tiles = (d_ub + 31) / 32;
+            k_theta_batch<T><<<dim3(tiles, tiles, nref), 256, 0, s>>>(insts, refs);
+        }
+    } else {
+        const int tiles = (d_ub + 31) / 32;
+        k_theta_batch<T><<<dim3(tiles, tiles, nref), 256, 0, s>>>(insts, refs);
+    }
     TQ_CHECK(cudaGetLastError());
     const int rows_cap = ((rows_ub + 7) & ~7) < 8 ? 8 : ((rows_ub + 7) & ~7);
     int rpl = 1;
@@ -2298,7 +2307,7 @@ void launch_entropy_batch(const InstTask<T>* insts, int ninst, cudaStream_t s) {
     template void launch_amplitude<T>(const MpsView<T>&, const int8_t*, cplx_t<T>*, double*, cudaStream_t);   \
     template void launch_single_site_batch<T>(const InstTask<T>*, int, int, int, cudaStream_t);                \
     template void launch_update_batch<T>(const InstTask<T>*, const UpdRef*, int, int, int, int, cudaStream_t,  \
-                                         cudaEvent_t, cudaEvent_t);                                          \
+                                         cudaEvent_t, cudaEvent_t, bool);                                    \
     template void launch_entropy_batch<T>(const InstTask<T>*, int, cudaStream_t);                               \
     template bool launch_anneal_resident<T>(const InstTask<T>*, const GateOp*, const int*, const int*, int, int, \
                                             int, int*, int, cudaStream_t);

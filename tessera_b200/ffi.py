@@ -141,7 +141,8 @@ def problem_struct(h, ei, ej, ew, sa, sb, bias=None, sc=None):
 
 
 def config_struct(dt=0.1, chi=32, precision="c128", zz_substeps=1, jacobi_tol=0.0, jacobi_max_sweeps=0,
-                  jacobi_block=0, device=-1, step_begin=0, step_end=0, initial_mps=None, skip_observables=False):
+                  jacobi_block=0, device=-1, step_begin=0, step_end=0, initial_mps=None, skip_observables=False,
+                  theta_tensor_cores=False):
     L = _lib.load()
     c = _lib.Config()
     L.tessera_qa_config_init(C.byref(c))
@@ -163,6 +164,7 @@ def config_struct(dt=0.1, chi=32, precision="c128", zz_substeps=1, jacobi_tol=0.
             keep = np.frombuffer(initial_mps, dtype=np.uint8).copy()
         c.initial_mps = keep.ctypes.data
     c.skip_observables = 1 if skip_observables else 0
+    c.theta_tensor_cores = 1 if theta_tensor_cores else 0
     return c, keep
 
 

@@ -327,3 +327,32 @@ def test_large_theta_batch_matches_cooperative_sessions(prec, n, chi, q0, tol, b
         assert 1 - fidelity(x, y) < tol, (prec, b)
         assert np.vdot(y, y).real == pytest.approx(np.vdot(x, x).real, rel=tol)
     sb.close()
+
+
+@pytest.mark.parametrize("batched", [False, True])
+def test_tensor_core_theta_matches_cuda_core_theta(batched):
+    """complex64 with theta_tensor_cores: the bond contraction runs on tcgen05 (split-TF32, FP32
+    accumulators in tensor memory).  Same gate slots, same random saturated MPS (chi=128, so the
+    contraction tiles are full 64 x 64 blocks, and chi-limited edge bonds give ragged ones): the
+    states agree with the CUDA-core FP32 contraction to FP32 rounding."""
+    p = instances.chain_range(n=16, dmax=3, seed=6, T=1.0, dt=0.05, chi=128)
+
+    def run(tc):
+        if batched:
+            s = ffi.Session.batch([p], chi=128, precision="c64", theta_tensor_cores=tc)
+        else:
+            s = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=128, precision="c64",
+                            theta_tensor_cores=tc)
+        s.randomize(21)
+        s.run_gates(5, 0, 72)
+        r = s.sync()
+        ck = s.save_instance(0) if batched else s.save()
+        s.close()
+        return r, ffi.sites_to_dense(ffi.checkpoint_to_sites(ck)[1])
+
+    r0, x = run(False)
+    r1, y = run(True)
+    assert r0.status == 0 and r1.status == 0
+    assert r0.two_site_updates == r1.two_site_updates == 72
+    assert 1 - fidelity(x, y) < 1e-8
+    assert np.vdot(y, y).real == pytest.approx(np.vdot(x, x).real, rel=1e-4)
