@@ -176,6 +176,31 @@ TESSERA_QA_API int tessera_qa_svd_noalloc(const double* d_a, size_t rows, size_t
 TESSERA_QA_API double tessera_qa_exact_ground(const double* h, size_t n, const size_t* ei, const size_t* ej,
                                               const double* ew, size_t m, int8_t* out_spins);
 
+/* ---- exact state-vector anneal on the GPU (rust/src/quantum.rs:63-112), 1 <= n <= 30 ----
+ * mode 0: the reference's splitting (quantum.rs:82-84): problem phase B dt/2, exp(+i A dt X) on
+ *         every qubit, problem phase B dt/2.
+ * mode 1: the MPS engine's splitting: single-site half steps exp(-i dt/2 (-A X - B h Z)) (with
+ *         the problem's warm-start field when it has one), the exact ZZ block, half steps again.
+ * |+>^n start, FP64 throughout, qubit-0 entropy per step (quantum.rs:138-175).  spins = the most
+ * probable pattern (quantum.rs:94-103, first maximum); sign_spins = the sign<Z> pattern.
+ * Memory: 32 bytes per basis state on the device. */
+typedef struct tessera_qa_sv_result {
+    int8_t* spins;          /* n, required */
+    int8_t* sign_spins;     /* n, optional */
+    double* entropy;        /* steps, optional */
+    double* state;          /* 2 * 2^n doubles (interleaved complex), optional */
+    double energy;          /* Ising energy of spins */
+    double expected_energy; /* <psi|H_problem|psi> / <psi|psi> */
+    double prob;            /* probability of spins */
+    double sign_energy;     /* Ising energy of sign_spins */
+    double sign_prob;       /* its probability (when state was requested, else -1) */
+    double norm2;           /* <psi|psi> */
+    double device_ms;
+    double reserved[4];
+} tessera_qa_sv_result;
+TESSERA_QA_API int tessera_qa_sv_anneal(const tessera_qa_problem* problem, double dt, int mode,
+                                        tessera_qa_sv_result* result);
+
 /* ---- learned schedules: a message-passing GNN trained and run by the library's own kernels ----
  * No counterpart in the reference's engine; python/gnn_guide.py:81-135 (its warm-start spin
  * predictor) is the architectural starting point.  From an Ising graph it predicts `knots`

@@ -53,6 +53,13 @@ _lib = None
 _lock = threading.Lock()
 
 
+class SvResult(C.Structure):
+    _fields_ = [("spins", c_int8_p), ("sign_spins", c_int8_p), ("entropy", c_double_p), ("state", c_double_p),
+                ("energy", C.c_double), ("expected_energy", C.c_double), ("prob", C.c_double),
+                ("sign_energy", C.c_double), ("sign_prob", C.c_double), ("norm2", C.c_double),
+                ("device_ms", C.c_double), ("reserved", C.c_double * 4)]
+
+
 def load(path: str = LIB_PATH) -> C.CDLL:
     """Load libtessera_qa.so (building it first if the sources are newer)."""
     global _lib
@@ -108,6 +115,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.tessera_qa_session_load.restype = C.c_int
         L.tessera_qa_session_save_instance.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t]
         L.tessera_qa_session_save_instance.restype = C.c_int
+        L.tessera_qa_sv_anneal.argtypes = [C.POINTER(Problem), C.c_double, C.c_int, C.POINTER(SvResult)]
+        L.tessera_qa_sv_anneal.restype = C.c_int
         L.tessera_qa_session_destroy.argtypes = [C.c_void_p]
         L.tessera_qa_session_destroy.restype = None
         _lib = L

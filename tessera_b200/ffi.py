@@ -371,6 +371,43 @@ class Session:
             pass
 
 
+@dataclass
+class SvAnnealResult:
+    spins: np.ndarray          # most probable pattern
+    sign_spins: np.ndarray     # sign<Z> pattern
+    energy: float
+    expected_energy: float
+    prob: float
+    sign_energy: float
+    entropy: np.ndarray
+    norm2: float
+    device_ms: float
+    state: np.ndarray | None = None
+
+
+def sv_anneal(h, ei, ej, ew, sa, sb, dt=0.1, mode=0, bias=None, sc=None, want_state=False) -> SvAnnealResult:
+    """tessera_qa_sv_anneal: the exact 2^n state-vector anneal on the GPU (rust/src/quantum.rs:63-112).
+    mode 0 = quantum.rs's splitting, mode 1 = the MPS engine's splitting."""
+    L = _lib.load()
+    P, keep = problem_struct(h, ei, ej, ew, sa, sb, bias, sc)
+    n, steps = int(P.n), int(P.steps)
+    spins = np.zeros(n, np.int8)
+    sspins = np.zeros(n, np.int8)
+    ent = np.zeros(steps)
+    st = np.zeros(2 << n) if want_state else None
+    r = _lib.SvResult()
+    r.spins = _p(spins, _lib.c_int8_p)
+    r.sign_spins = _p(sspins, _lib.c_int8_p)
+    r.entropy = _p(ent, _lib.c_double_p)
+    if st is not None:
+        r.state = _p(st, _lib.c_double_p)
+    rc = L.tessera_qa_sv_anneal(C.byref(P), dt, mode, C.byref(r))
+    if rc != 0:
+        raise _lib.EngineError(rc, _lib.last_error())
+    return SvAnnealResult(spins, sspins, r.energy, r.expected_energy, r.prob, r.sign_energy, ent, r.norm2,
+                          r.device_ms, st.view(np.complex128) if st is not None else None)
+
+
 def anneal_batch(problems, dt=None, chi=None, precision="c128", zz_substeps=1, want_checkpoint=False,
                  raise_on_status=True, skip_observables=False, jacobi_block=0, device=-1):
     """tessera_qa_anneal_batch over a list of instances.Problem (each uses its own dt and chi unless
