@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--dmax", type=int, default=4)
     ap.add_argument("--chi", type=int, default=256)
     ap.add_argument("--jacobi-block", type=int, default=0)
+    ap.add_argument("--theta-tc", action="store_true",
+                    help="complex64: bond contraction on the tcgen05 tensor cores (split-TF32)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-solves", action="store_true", help="skip the solves/s (chosen vs plain) measurement")
@@ -347,7 +349,7 @@ def main():
                            jacobi_block=args.jacobi_block, kernel_timing=True, device=local)
     else:
         sess = ffi.Session.batch(probs, chi=args.chi, precision=args.precision, jacobi_block=args.jacobi_block,
-                                 kernel_timing=True, device=local)
+                                 kernel_timing=True, device=local, theta_tensor_cores=args.theta_tc)
     sess.randomize(1234 + 1000 * rank)
     G = upd_per_step_inst
     # Gate slots of edges (i, i+d) with 32 <= i < 96: every bond they touch sits at chi = 256
