@@ -1525,6 +1525,8 @@ __global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd(MpsView<T> mps
 // 2 (P-1) P/2 times, and no copy waits in the open.  Every pair is visited once per sweep
 // (a cyclic ordering), with the rotation of jacobi_rotation.
 // ------------------------------------------------------------------------------------
+constexpr int RC_MAXB = 256;  // column blocks of one theta (N <= 256 BW)
+
 template <typename T>
 __device__ __forceinline__ void rc_stage(cplx_t<T>* dst, const cplx_t<T>* W, int ld, int rc, int R, int N, int blk,
                                          int BW, uint64_t* bar) {
@@ -1549,6 +1551,10 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
     __shared__ int s_rot;
     __shared__ int s_ok;
     __shared__ __align__(8) uint64_t bars[3];  // [0] block I, [1], [2] the two J buffers
+    // blocks modified in the previous sweep and so far in this one: a pair whose two blocks are
+    // unchanged since it was last found orthogonal is not checked again
+    __shared__ unsigned char mod_prev[RC_MAXB], mod_cur[RC_MAXB];
+    __shared__ int s_irot, s_jrot;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int R = pp.R > 0 ? pp.R : 2 * mps.dims[pp.bond];
     const int N = pp.N > 0 ? pp.N : 2 * mps.dims[pp.bond + 2];
@@ -1592,19 +1598,39 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
     const double tiny = noise_tiny(pp.tiny, R, fro2, sizeof(T) == 4);
     __syncthreads();
     const int nb = (N + BW - 1) / BW;
+    if (nb > RC_MAXB) {  // host sizing bug guard (N <= BW * RC_MAXB)
+        if (tid == 0) atomicOr(status, ST_BAD_DIMS);
+        return;
+    }
+    for (int e = tid; e < nb; e += NT) { mod_prev[e] = 1; mod_cur[e] = 1; }
     double rots_total = 0.0;
+    double pairs_checked = 0.0;
+    double moved = 2.0 * nb;  // column blocks read or written (the norm passes: one read each)
+    // first block J > j0 whose pair with I needs a check (nb: none)
+    auto next_needed = [&](int j0, bool iflag) {
+        int j = j0;
+        while (j < nb && !(iflag || mod_prev[j] || mod_cur[j])) ++j;
+        return j;
+    };
     int sweep = 0;
     bool converged = false;
     bool fail = false;
     for (; sweep < pp.max_sweeps && !fail; ++sweep) {
         if (tid == 0) s_rot = 0;
         __syncthreads();
+        for (int e = tid; e < nb; e += NT) { mod_prev[e] = mod_cur[e]; mod_cur[e] = 0; }
+        __syncthreads();
         int rot = 0;
         for (int I = 0; I < nb && !fail; ++I) {
-            if (tid == 0) rc_stage<T>(ci, W, ld, rc, R, N, I, BW, &bars[0]);
+            const bool iflag = mod_prev[I] || mod_cur[I];
+            int jn = next_needed(I + 1, iflag);
+            if (!iflag && jn >= nb) continue;  // every pair of block I is unchanged and orthogonal
+            if (tid == 0) { s_irot = 0; rc_stage<T>(ci, W, ld, rc, R, N, I, BW, &bars[0]); }
+            moved += 1.0;
             if (!wait(0)) { fail = true; break; }
             // inner pairs of block I: circle method, BW/2 pairs per round, G2 threads each
-            {
+            if (iflag) {
+                pairs_checked += 0.5 * BW * (BW - 1);
                 const int ip = tid / G2;
                 for (int t = 0; t < BW - 1; ++t) {
                     int x, y;
@@ -1612,7 +1638,7 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
                     else { x = (t + ip) % (BW - 1); y = (t - ip + (BW - 1)) % (BW - 1); }
                     const bool ok = (I * BW + x < N) && (I * BW + y < N);
                     const int r1 = rotate_pair<T, G2>(ci + x * rc, ci + y * rc, ok, R, pp.tol, tiny, red, tid);
-                    if (r1 && (tid % G2) == 0) ++rot;
+                    if (r1 && (tid % G2) == 0) { ++rot; s_irot = 1; }
                     __syncthreads();
                 }
             }
@@ -1624,11 +1650,15 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
                 xi[k] = row < R ? ci[warp * rc + row] : czero<V>();
             }
             __syncthreads();  // ci free for the next block I
-            if (I + 1 < nb && tid == 0) rc_stage<T>(cj[0], W, ld, rc, R, N, I + 1, BW, &bars[1]);
-            for (int J = I + 1; J < nb; ++J) {
-                const int b = (J - I - 1) & 1;
-                if (J + 1 < nb && tid == 0) rc_stage<T>(cj[b ^ 1], W, ld, rc, R, N, J + 1, BW, &bars[1 + (b ^ 1)]);
+            if (jn < nb && tid == 0) rc_stage<T>(cj[0], W, ld, rc, R, N, jn, BW, &bars[1]);
+            int b = 0;
+            for (int J = jn; J < nb; J = jn, b ^= 1) {
+                jn = next_needed(J + 1, iflag);
+                if (jn < nb && tid == 0) rc_stage<T>(cj[b ^ 1], W, ld, rc, R, N, jn, BW, &bars[1 + (b ^ 1)]);
+                if (tid == 0) s_jrot = 0;
                 if (!wait(1 + b)) { fail = true; break; }
+                pairs_checked += (double)BW * BW;
+                moved += 1.0;
                 V* cb = cj[b];
                 for (int t = 0; t < BW; ++t) {
                     const int q = (warp + t) % BW;
@@ -1671,22 +1701,29 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
                             const int row = lane + 32 * k;
                             if (row < R) cq[row] = yj[k];
                         }
-                        if (lane == 0) ++rot;
+                        if (lane == 0) { ++rot; s_jrot = 1; s_irot = 1; }
                     }
                     __syncthreads();
                 }
-                // block J back to global memory; later bulk copies read it
-                for (int c = warp; c < BW; c += NW) {
-                    if (J * BW + c >= N) continue;
-                    V* dst = W + (long long)(J * BW + c) * ld;
-                    const V* src = cb + c * rc;
-                    for (int row = lane; row < R; row += 32) dst[row] = src[row];
+                // block J back to global memory when it changed; later bulk copies read it
+                if (s_jrot) {
+                    moved += 1.0;
+                    if (tid == 0) mod_cur[J] = 1;
+                    for (int c = warp; c < BW; c += NW) {
+                        if (J * BW + c >= N) continue;
+                        V* dst = W + (long long)(J * BW + c) * ld;
+                        const V* src = cb + c * rc;
+                        for (int row = lane; row < R; row += 32) dst[row] = src[row];
+                    }
+                    fence_proxy_async_global();
                 }
-                fence_proxy_async_global();
                 __syncthreads();
             }
             if (fail) break;
-            if (vi) {
+            const bool i_changed = s_irot != 0;
+            if (i_changed && tid == 0) mod_cur[I] = 1;
+            if (i_changed) moved += 1.0;
+            if (vi && i_changed) {
                 V* dst = W + (long long)(I * BW + warp) * ld;
 #pragma unroll
                 for (int k = 0; k < RPL; ++k) {
@@ -1727,9 +1764,8 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
         if (lane == 0) wk.sig2[j] = sj;
     }
     __syncthreads();
-    const double moves = (double)sweep * ((double)nb + 0.5 * nb * (nb - 1)) * 2.0 + 2.0;
-    const double flops = (double)sweep * 0.5 * N * (N - 1) * R * 16.0 + rots_total * R * 32.0;
-    svd_finish<T>(mps, wk, pp, R, N, fmax(1e-28, tiny), sweep, converged, moves * (double)BW * R * sizeof(V), smraw,
+    const double flops = pairs_checked * R * 16.0 + rots_total * R * 32.0;
+    svd_finish<T>(mps, wk, pp, R, N, fmax(1e-28, tiny), sweep, converged, moved * (double)BW * R * sizeof(V), smraw,
                   red, flops);
 }
 
