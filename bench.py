@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--jacobi-block", type=int, default=0)
     ap.add_argument("--theta-tc", action="store_true",
                     help="complex64: bond contraction on the tcgen05 tensor cores (split-TF32)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="time the batched Jacobi kernels (and, in complex64, the tensor-core contraction) on a "
+                         "slice of this workload first and run the fastest (tessera_b200.autotune)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-solves", action="store_true", help="skip the solves/s (chosen vs plain) measurement")
@@ -343,6 +346,13 @@ def main():
     B = max(1, args.batch)
     probs = [workload(args, i) for i in shard(rank, B)]
     p = probs[0]
+    tuned = None
+    if args.autotune and B > 1:
+        from tessera_b200 import autotune
+        ch = autotune.tune(probs, args.chi, args.precision)
+        args.jacobi_block, args.theta_tc = ch.jacobi_block, ch.theta_tensor_cores
+        tuned = {"jacobi_block": ch.jacobi_block, "theta_tensor_cores": ch.theta_tensor_cores,
+                 "measured_ms_per_update": {k: v["ms_per_update"] for k, v in ch.measured.items()}}
     upd_per_step_inst = min(args.gates, p.updates_per_step())
     if B == 1:
         sess = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=args.chi, precision=args.precision,
@@ -495,6 +505,7 @@ def main():
 
     if rank == 0:
         cfg = config_dict(args, p)
+        cfg.update({"jacobi_block": args.jacobi_block, "theta_tensor_cores": bool(args.theta_tc), "autotune": tuned})
         cfg.update({"instances_per_gpu": B, "gates_per_step": G,
                     "step": f"{G} consecutive gate slots of the Trotter step at s=0.5 on each of {B} instances"})
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -1,0 +1,105 @@
+"""Measured choice of the batched Jacobi kernel for a workload (the engine's autotuner).
+
+The batched engine has three SVD kernels for a large theta (the block-row-cyclic column-pair
+Jacobi with blocks of 4 or 8 columns, and the block-Gram Jacobi) and, for complex64, two bond
+contractions (CUDA cores or tcgen05 tensor cores).  Which is fastest depends on the bond
+dimension, the precision and how many instances share the GPU.  ``tune`` times each candidate
+on the workload itself: a batched session of the given instances, each MPS a seeded random state
+with every bond at its cap, a few interior gate slots per candidate, CUDA events around them.
+The choice is cached in a JSON file keyed by (chi, precision, instance count, GPU name), so a
+later run of the same workload reuses it without measuring.
+
+Every candidate computes the same rotations to rounding; the choice changes speed, not results
+beyond rounding.
+"""
+from __future__ import annotations
+
+import json
+import os
+import time
+from dataclasses import asdict, dataclass
+
+from . import ffi
+
+CACHE = os.path.join(os.path.expanduser("~"), ".cache", "tessera_b200", "autotune.json")
+
+
+@dataclass
+class Choice:
+    jacobi_block: int
+    theta_tensor_cores: bool
+    ms_per_update: float
+    measured: dict
+
+
+def _gpu_name() -> str:
+    try:
+        import torch
+        return torch.cuda.get_device_name(0)
+    except Exception:
+        return "unknown"
+
+
+def candidates(precision: str):
+    out = [(8, False), (4, False), (32, False)]
+    if precision == "c64":
+        out.append((8, True))
+    return out
+
+
+def _time_candidate(problems, chi, precision, block, tc, q0, gates, seed=1234):
+    s = ffi.Session.batch(problems, chi=chi, precision=precision, jacobi_block=block, theta_tensor_cores=tc)
+    try:
+        s.randomize(seed)
+        k = problems[0].steps // 2
+        s.run_gates(k, q0, q0 + 1)  # warm-up slot (kernel load, caches)
+        s.sync()
+        s.run_gates(k, q0 + 1, q0 + 1 + gates)
+        r = s.sync()
+        if r.status:
+            return None
+        return r.device_ms / max(1, gates * len(problems))
+    finally:
+        s.close()
+
+
+def tune(problems, chi: int, precision: str = "c128", gates: int = 2, q0: int | None = None, cache: str | None = CACHE,
+         force: bool = False) -> Choice:
+    """Fastest (jacobi_block, theta_tensor_cores) for a batched run of `problems` at bond cap `chi`."""
+    key = f"chi={chi}|{precision}|B={len(problems)}|{_gpu_name()}"
+    if cache and not force and os.path.exists(cache):
+        try:
+            with open(cache) as f:
+                d = json.load(f)
+            if key in d:
+                return Choice(**d[key])
+        except Exception:
+            pass
+    n = problems[0].n
+    if q0 is None:
+        q0 = 16 * min(32, n // 4)  # interior gate slots (saturated bonds for long chains)
+    measured = {}
+    for block, tc in candidates(precision):
+        t0 = time.perf_counter()
+        ms = _time_candidate(problems, chi, precision, block, tc, q0, gates)
+        measured[f"block={block},tc={int(tc)}"] = {"ms_per_update": ms, "wall_s": time.perf_counter() - t0}
+    ok = {k: v["ms_per_update"] for k, v in measured.items() if v["ms_per_update"] is not None}
+    if not ok:
+        raise RuntimeError("no Jacobi kernel candidate ran cleanly on this workload")
+    best = min(ok, key=ok.get)
+    block = int(best.split(",")[0].split("=")[1])
+    tc = best.endswith("tc=1")
+    choice = Choice(block, tc, ok[best], measured)
+    if cache:
+        try:
+            os.makedirs(os.path.dirname(cache), exist_ok=True)
+            d = {}
+            if os.path.exists(cache):
+                with open(cache) as f:
+                    d = json.load(f)
+            d[key] = asdict(choice)
+            with open(cache, "w") as f:
+                json.dump(d, f, indent=1)
+        except Exception:
+            pass
+    return choice

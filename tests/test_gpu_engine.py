@@ -380,3 +380,13 @@ def test_exact_chi256_state_matches_statevector(oracle, batched):
     assert 1 - fidelity(psi, sv.state) < 1e-8
     assert r.expected_energy == pytest.approx(sv.expected_energy, abs=1e-8)
     assert int(np.argmax(np.abs(psi) ** 2)) == int(np.argmax(np.abs(sv.state) ** 2))
+
+
+def test_autotuner_times_every_candidate_and_picks_the_fastest():
+    from tessera_b200 import autotune
+    probs = [instances.chain_range(n=24, dmax=2, seed=s, T=1.0, dt=0.05, chi=64) for s in (1, 2, 3)]
+    ch = autotune.tune(probs, 64, "c64", gates=2, cache=None)
+    assert len(ch.measured) == len(autotune.candidates("c64"))
+    times = {k: v["ms_per_update"] for k, v in ch.measured.items() if v["ms_per_update"] is not None}
+    assert ch.ms_per_update == min(times.values())
+    assert (ch.jacobi_block, ch.theta_tensor_cores) in autotune.candidates("c64")
