@@ -269,6 +269,13 @@ TESSERA_QA_API int tessera_qa_session_observe(tessera_qa_session* s, tessera_qa_
 /* Writes / reads a checkpoint of the current state. */
 TESSERA_QA_API int tessera_qa_session_save(tessera_qa_session* s, void* buf, size_t bytes);
 TESSERA_QA_API int tessera_qa_session_load(tessera_qa_session* s, const void* buf, size_t bytes);
+/* Draws `count` basis patterns x from |<x|psi>|^2 / <psi|psi> of the session's MPS (perfect
+ * sampling, site by site with the right environments): out_spins count x n (+1/-1), and the
+ * Ising energy of each in out_energies (may be NULL).  The readout for instances whose <Z_i>
+ * vanish (h = 0), where the sign readout of cuda/src/mps.cpp:370-371 carries no information.
+ * Single-instance sessions; deterministic for a given seed. */
+TESSERA_QA_API int tessera_qa_session_sample(tessera_qa_session* s, size_t count, uint64_t seed, int8_t* out_spins,
+                                             double* out_energies);
 /* Checkpoint of one instance of a batched session (index 0 for a single-instance session). */
 TESSERA_QA_API int tessera_qa_session_save_instance(tessera_qa_session* s, size_t index, void* buf, size_t bytes);
 TESSERA_QA_API void tessera_qa_session_destroy(tessera_qa_session* s);

@@ -115,6 +115,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.tessera_qa_session_load.restype = C.c_int
         L.tessera_qa_session_save_instance.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t]
         L.tessera_qa_session_save_instance.restype = C.c_int
+        L.tessera_qa_session_sample.argtypes = [C.c_void_p, C.c_size_t, C.c_uint64, c_int8_p, c_double_p]
+        L.tessera_qa_session_sample.restype = C.c_int
         L.tessera_qa_sv_anneal.argtypes = [C.POINTER(Problem), C.c_double, C.c_int, C.POINTER(SvResult)]
         L.tessera_qa_sv_anneal.restype = C.c_int
         L.tessera_qa_session_destroy.argtypes = [C.c_void_p]

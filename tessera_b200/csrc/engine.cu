@@ -177,6 +177,7 @@ public:
     virtual void set_values(const ProblemHost& P) = 0;
     virtual void sync_stats(tessera_qa_result* r) = 0;
     virtual void observe(tessera_qa_result* r) = 0;
+    virtual void sample(size_t count, unsigned long long seed, int8_t* spins, double* energies) = 0;
     virtual size_t save(void* buf, size_t bytes, unsigned long long step_next) = 0;
     virtual void load(const void* buf, size_t bytes) = 0;
     virtual void copy_entropy(double* out, int k0, int k1) = 0;
@@ -388,6 +389,41 @@ public:
             if (r->spins) std::memcpy(r->spins, spins.data(), n_);
             if (r->z_expect) std::memcpy(r->z_expect, ez.data(), sizeof(double) * n_);
         }
+    }
+
+    // `count` basis patterns drawn from |<x|psi>|^2 (K9), their Ising energies on the host
+    void sample(size_t count, unsigned long long seed, int8_t* spins, double* energies) override {
+        if (count == 0) return;
+        if (count > (size_t)1 << 24) throw ArgError("at most 2^24 samples per call");
+        const MpsView<T> M = mps();
+        if (!obs_) {
+            const size_t bytes = sizeof(V) * (size_t)cap_ * cap_ * obs_units_;
+            TQ_CK(cudaMalloc(&obs_, bytes));
+            V one = mk<V>(1, 0);
+            TQ_CK(cudaMemcpyAsync(obs_, &one, sizeof(V), cudaMemcpyHostToDevice, stream_));
+        }
+        launch_chain<T>(M, 1, obsR_, n_, obs_, xs_, bar_, stats_, cap_, stream_);
+        int8_t* d = nullptr;
+        TQ_CK(cudaMalloc(&d, count * (size_t)n_));
+        cudaError_t err = cudaSuccess;
+        try {
+            launch_sample<T>(M, obs_, (int)count, seed, d, stream_);
+        } catch (...) {
+            cudaFree(d);
+            throw;
+        }
+        err = cudaMemcpyAsync(spins, d, count * (size_t)n_, cudaMemcpyDeviceToHost, stream_);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(stream_);
+        cudaFree(d);
+        TQ_CK(err);
+        if (energies)
+            for (size_t c = 0; c < count; ++c) {
+                const int8_t* x = spins + c * n_;
+                double e = 0.0;
+                for (int q = 0; q < m_; ++q) e -= P_.w[q] * x[P_.ei[q]] * x[P_.ej[q]];
+                for (int i = 0; i < n_; ++i) e -= P_.h[i] * x[i];
+                energies[c] = e;
+            }
     }
 
     size_t save(void* buf, size_t bytes, unsigned long long step_next) override {
@@ -1432,6 +1468,17 @@ int tessera_qa_session_save_instance(tessera_qa_session* s, size_t index, void* 
             if (index != 0) throw ArgError("instance index out of range");
             s->eng->save(buf, bytes, 0);
         }
+        return 0;
+    });
+}
+
+int tessera_qa_session_sample(tessera_qa_session* s, size_t count, uint64_t seed, int8_t* out_spins,
+                              double* out_energies) {
+    return guarded([&]() -> int {
+        if (!s) throw ArgError("session is NULL");
+        if (s->batch) throw ArgError("sampling is per instance: use a single-instance session");
+        if (count && !out_spins) throw ArgError("out_spins is NULL");
+        s->eng->sample(count, (unsigned long long)seed, out_spins, out_energies);
         return 0;
     });
 }

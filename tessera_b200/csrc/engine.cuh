@@ -168,6 +168,10 @@ void launch_entropy_batch(const InstTask<T>* insts, int ninst, cudaStream_t s);
 template <typename T>
 bool launch_anneal_resident(const InstTask<T>* insts, const GateOp* ops, const int* op_off, const int* order,
                             int ninst, int k0, int k1, int* work, int rows_cap, cudaStream_t s);
+// perfect sampling of basis patterns from the MPS with the right environments in `envs`
+template <typename T>
+void launch_sample(const MpsView<T>& mps, const cplx_t<T>* envs, int count, unsigned long long seed, int8_t* out,
+                   cudaStream_t s);
 // complex64 bond contraction on tcgen05 tensor cores, split-TF32 (theta_tc.cu)
 bool theta_tc_supported(const GateOp& op);
 void launch_theta_tc(const MpsView<float>& mps, const ScheduleView& sch, GateOp op, SvdWork<float> wk, int dl_ub,

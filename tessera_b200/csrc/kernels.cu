@@ -2197,6 +2197,105 @@ void launch_amplitude(const MpsView<T>& mps, const int8_t* spins, cplx_t<T>* scr
 }
 
 // ------------------------------------------------------------------------------------
+// K9: perfect sampling of basis patterns x with probability |<x|psi>|^2 / <psi|psi> from the
+// MPS, site by site: with the left vector v = A_0^{s_0} ... A_{i-1}^{s_{i-1}} (rescaled) and
+// the right environment R_{i+1} (the observables' chain), w_s = v A_i^s and
+// p(s_i = s | s_<i) ~ w_s R_{i+1} w_s^dagger.  One CTA per sample, FP64 sums, a counter-based
+// splitmix64 stream per (seed, sample, site).  Replaces the sign<Z> readout where it is
+// undefined (Z2-symmetric instances, <Z_i> = 0).
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ double sample_uniform(unsigned long long seed, int smp, int site) {
+    unsigned long long x = seed + 0x9E3779B97F4A7C15ull * (unsigned long long)(smp + 1) +
+                           0xD1B54A32D192ED03ull * (unsigned long long)(site + 1);
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    x ^= x >> 31;
+    return (double)(x >> 11) * (1.0 / 9007199254740992.0);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_sample(MpsView<T> mps, const cplx_t<T>* envs, int count,
+                                                unsigned long long seed, int8_t* out) {
+    using V = cplx_t<T>;
+    extern __shared__ double2 sbuf[];  // v, w0, w1: cap complex each
+    __shared__ double red[2][8];
+    __shared__ double s_scale;
+    __shared__ int s_pick;
+    const int tid = threadIdx.x, NT = blockDim.x;
+    const int n = mps.n, cap = mps.cap;
+    double2* v = sbuf;
+    double2* w0 = v + cap;
+    double2* w1 = w0 + cap;
+    const long long U = (long long)cap * cap;
+    for (int smp = blockIdx.x; smp < count; smp += gridDim.x) {
+        if (tid == 0) v[0] = make_double2(1.0, 0.0);
+        __syncthreads();
+        for (int i = 0; i < n; ++i) {
+            const int dl = mps.dims[i], dr = mps.dims[i + 1];
+            const V* A = mps.site(i);
+            for (int b = tid; b < dr; b += NT) {
+                double2 a0 = make_double2(0, 0), a1 = make_double2(0, 0);
+                for (int a = 0; a < dl; ++a) {
+                    const double2 va = v[a];
+                    const V x0 = A[(long long)(2 * a) * cap + b], x1 = A[(long long)(2 * a + 1) * cap + b];
+                    a0.x += va.x * x0.x - va.y * x0.y; a0.y += va.x * x0.y + va.y * x0.x;
+                    a1.x += va.x * x1.x - va.y * x1.y; a1.y += va.x * x1.y + va.y * x1.x;
+                }
+                w0[b] = a0;
+                w1[b] = a1;
+            }
+            __syncthreads();
+            const V* Rm = envs + (i + 1 == n ? 0LL : (1LL + n + i + 1) * U);  // R_{i+1}; R_n = 1
+            double p0 = 0.0, p1 = 0.0;
+            for (int b = tid; b < dr; b += NT) {
+                double2 t0 = make_double2(0, 0), t1 = make_double2(0, 0);  // sum_b' R[b, b'] conj(w[b'])
+                for (int bp = 0; bp < dr; ++bp) {
+                    const V r = Rm[(long long)b * cap + bp];
+                    const double2 c0 = w0[bp], c1 = w1[bp];
+                    t0.x += r.x * c0.x + r.y * c0.y; t0.y += r.y * c0.x - r.x * c0.y;
+                    t1.x += r.x * c1.x + r.y * c1.y; t1.y += r.y * c1.x - r.x * c1.y;
+                }
+                p0 += w0[b].x * t0.x - w0[b].y * t0.y;
+                p1 += w1[b].x * t1.x - w1[b].y * t1.y;
+            }
+            p0 = warp_sum(p0);
+            p1 = warp_sum(p1);
+            if ((tid & 31) == 0) { red[0][tid >> 5] = p0; red[1][tid >> 5] = p1; }
+            __syncthreads();
+            if (tid == 0) {
+                double q0 = 0, q1 = 0;
+                for (int w = 0; w < (NT >> 5); ++w) { q0 += red[0][w]; q1 += red[1][w]; }
+                q0 = fmax(q0, 0.0);
+                q1 = fmax(q1, 0.0);
+                const double tot = q0 + q1;
+                const int pick = (tot > 0 && sample_uniform(seed, smp, i) * tot >= q0) ? 1 : 0;
+                s_pick = pick;
+                const double pp = pick ? q1 : q0;
+                s_scale = pp > 0 ? 1.0 / sqrt(pp) : 1.0;
+                out[(long long)smp * n + i] = pick ? -1 : 1;  // physical 0 <-> spin +1
+            }
+            __syncthreads();
+            const double2* wc = s_pick ? w1 : w0;
+            const double sc = s_scale;
+            for (int b = tid; b < dr; b += NT) v[b] = make_double2(wc[b].x * sc, wc[b].y * sc);
+            __syncthreads();
+        }
+    }
+}
+
+template <typename T>
+void launch_sample(const MpsView<T>& mps, const cplx_t<T>* envs, int count, unsigned long long seed, int8_t* out,
+                   cudaStream_t s) {
+    const size_t smem = sizeof(double2) * 3 * (size_t)mps.cap;
+    auto fn = k_sample<T>;
+    if (smem > 48 * 1024) TQ_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int grid = 4 * num_sms();
+    if (grid > count) grid = count;
+    fn<<<grid, 256, smem, s>>>(mps, envs, count, seed, out);
+    TQ_CHECK(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------------------------
 // Batched kernels: many instances (each with its own MPS, workspace and statistics) in
 // one launch.  Every instance keeps its own gate order; a launch runs gate q of every
 // instance that has one.
@@ -2345,6 +2444,8 @@ void launch_entropy_batch(const InstTask<T>* insts, int ninst, cudaStream_t s) {
     template void launch_update_batch<T>(const InstTask<T>*, const UpdRef*, int, int, int, int, cudaStream_t,  \
                                          cudaEvent_t, cudaEvent_t, bool);                                    \
     template void launch_entropy_batch<T>(const InstTask<T>*, int, cudaStream_t);                               \
+    template void launch_sample<T>(const MpsView<T>&, const cplx_t<T>*, int, unsigned long long, int8_t*,       \
+                                   cudaStream_t);                                                              \
     template bool launch_anneal_resident<T>(const InstTask<T>*, const GateOp*, const int*, const int*, int, int, \
                                             int, int*, int, cudaStream_t);
 TQ_INST(double)

@@ -345,6 +345,15 @@ class Session:
         self._ck(self._L.tessera_qa_session_save(self._h, buf.ctypes.data, nb))
         return buf.tobytes()
 
+    def sample(self, count: int, seed: int = 0):
+        """(spins (count, n) int8, energies (count,)): patterns drawn from |<x|psi>|^2
+        (tessera_qa_session_sample)."""
+        spins = np.zeros((count, self.n), np.int8)
+        en = np.zeros(count)
+        self._ck(self._L.tessera_qa_session_sample(self._h, count, seed, spins.ctypes.data_as(_lib.c_int8_p),
+                                                   en.ctypes.data_as(_lib.c_double_p)))
+        return spins, en
+
     def save_instance(self, index: int) -> bytes:
         """Checkpoint of instance `index` of a batched session (tessera_qa_session_save_instance)."""
         nb = self._L.tessera_qa_checkpoint_bytes(self.n_of(index), self.chi)

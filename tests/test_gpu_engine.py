@@ -392,3 +392,31 @@ def test_autotuner_times_every_candidate_and_picks_the_fastest():
     times = {k: v["ms_per_update"] for k, v in ch.measured.items() if v["ms_per_update"] is not None}
     assert len(times) == len(ch.measured) and ch.ms_per_update == min(times.values())
     assert (ch.jacobi_block, ch.theta_tensor_cores) in autotune.candidates("c128")
+
+
+def test_mps_sampling_matches_state_probabilities():
+    """tessera_qa_session_sample draws patterns with the MPS's own probabilities: on an n=8
+    exact-chi anneal the empirical frequencies of the most probable patterns agree with
+    |<x|psi>|^2 / <psi|psi> within 5 standard errors, the total variation distance is small,
+    the energies belong to the patterns, and a seed reproduces its draw."""
+    m = _rand_small(8, 4)
+    sa, sb = instances.linear(60)
+    s = ffi.Session(m.h, m.ei, m.ej, m.ew, sa, sb, dt=0.1, chi=16)
+    s.run(0, 60)
+    s.sync()
+    psi = ffi.sites_to_dense(ffi.checkpoint_to_sites(s.save())[1])
+    prob = np.abs(psi) ** 2 / np.vdot(psi, psi).real
+    N = 40000
+    spins, en = s.sample(N, seed=7)
+    idx = ((spins == -1).astype(np.int64) << np.arange(8)).sum(axis=1)
+    freq = np.bincount(idx, minlength=256) / N
+    for x in np.argsort(prob)[-10:]:
+        assert abs(freq[x] - prob[x]) < 5 * np.sqrt(prob[x] * (1 - prob[x]) / N) + 1e-3, (x, freq[x], prob[x])
+    assert 0.5 * np.abs(freq - prob).sum() < 0.05
+    for k in range(20):
+        x = spins[k]
+        e = -sum(w * x[i] * x[j] for i, j, w in zip(m.ei, m.ej, m.ew)) - float(np.dot(m.h, x))
+        assert en[k] == pytest.approx(e, abs=1e-12)
+    again, _ = s.sample(100, seed=7)
+    assert np.array_equal(again, spins[:100])
+    s.close()
