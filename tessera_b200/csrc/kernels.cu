@@ -1525,11 +1525,11 @@ __global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd(MpsView<T> mps
 // 2 (P-1) P/2 times, and no copy waits in the open.  Every pair is visited once per sweep
 // (a cyclic ordering), with the rotation of jacobi_rotation.
 // ------------------------------------------------------------------------------------
-constexpr int RC_MAXB = 256;  // column blocks of one theta (N <= 256 BW)
+constexpr int RC_MAXN = 1024;  // columns of one theta in the block-row-cyclic kernel
 
 template <typename T>
 __device__ __forceinline__ void rc_stage(cplx_t<T>* dst, const cplx_t<T>* W, int ld, int rc, int R, int N, int blk,
-                                         int BW, uint64_t* bar) {
+                                         int BW, uint64_t* bar, const int* perm) {
     using V = cplx_t<T>;
     unsigned nv = 0;
     for (int c = 0; c < BW; ++c) nv += blk * BW + c < N;
@@ -1537,7 +1537,28 @@ __device__ __forceinline__ void rc_stage(cplx_t<T>* dst, const cplx_t<T>* W, int
     fence_proxy_async_shared();
     mbar_expect_tx(bar, nv * bytes);
     for (int c = 0; c < BW; ++c)
-        if (blk * BW + c < N) tma_load_1d(dst + c * rc, W + (long long)(blk * BW + c) * ld, bytes, bar);
+        if (blk * BW + c < N) tma_load_1d(dst + c * rc, W + (long long)perm[blk * BW + c] * ld, bytes, bar);
+}
+
+// descending bitonic sort of key[0..P2) carrying idx (ties: ascending idx); P2 a power of two
+__device__ void bitonic_desc(double* key, int* idx, int P2) {
+    const int tid = threadIdx.x, NT = blockDim.x;
+    for (int k = 2; k <= P2; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int e = tid; e < P2; e += NT) {
+                const int o = e ^ j;
+                if (o > e) {
+                    const bool desc = ((e & k) == 0);
+                    const double ke = key[e], ko = key[o];
+                    const int ie = idx[e], io = idx[o];
+                    const bool e_first = (ke > ko) || (ke == ko && ie < io);
+                    if (desc ? !e_first : e_first) {
+                        key[e] = ko; key[o] = ke; idx[e] = io; idx[o] = ie;
+                    }
+                }
+            }
+            __syncthreads();
+        }
 }
 
 template <typename T, int BW, int RPL>
@@ -1551,9 +1572,11 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
     __shared__ int s_rot;
     __shared__ int s_ok;
     __shared__ __align__(8) uint64_t bars[3];  // [0] block I, [1], [2] the two J buffers
-    // blocks modified in the previous sweep and so far in this one: a pair whose two blocks are
-    // unchanged since it was last found orthogonal is not checked again
-    __shared__ unsigned char mod_prev[RC_MAXB], mod_cur[RC_MAXB];
+    // columns modified in the previous sweep and so far in this one: a block pair whose columns
+    // are all unchanged since they were last found orthogonal is not checked again
+    __shared__ unsigned char cprev[RC_MAXN], ccur[RC_MAXN];
+    // this sweep's column order: descending norm (block position p holds column perm[p])
+    __shared__ int perm[RC_MAXN];
     __shared__ int s_irot, s_jrot;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int R = pp.R > 0 ? pp.R : 2 * mps.dims[pp.bond];
@@ -1598,34 +1621,68 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
     const double tiny = noise_tiny(pp.tiny, R, fro2, sizeof(T) == 4);
     __syncthreads();
     const int nb = (N + BW - 1) / BW;
-    if (nb > RC_MAXB) {  // host sizing bug guard (N <= BW * RC_MAXB)
+    if (N > RC_MAXN) {  // host sizing bug guard
         if (tid == 0) atomicOr(status, ST_BAD_DIMS);
         return;
     }
-    for (int e = tid; e < nb; e += NT) { mod_prev[e] = 1; mod_cur[e] = 1; }
+    for (int e = tid; e < N; e += NT) { cprev[e] = 1; ccur[e] = 1; }
     double rots_total = 0.0;
     double pairs_checked = 0.0;
     double moved = 2.0 * nb;  // column blocks read or written (the norm passes: one read each)
-    // first block J > j0 whose pair with I needs a check (nb: none)
+    auto blk_dirty = [&](int B) {
+        bool d = false;
+        for (int c = 0; c < BW; ++c) {
+            const int q = B * BW + c;
+            if (q < N) d = d || cprev[perm[q]] || ccur[perm[q]];
+        }
+        return d;
+    };
+    // first block J >= j0 whose pair with I needs a check (nb: none)
     auto next_needed = [&](int j0, bool iflag) {
         int j = j0;
-        while (j < nb && !(iflag || mod_prev[j] || mod_cur[j])) ++j;
+        while (j < nb && !(iflag || blk_dirty(j))) ++j;
         return j;
     };
+    int P2 = 1;
+    while (P2 < N) P2 <<= 1;
     int sweep = 0;
     bool converged = false;
     bool fail = false;
     for (; sweep < pp.max_sweeps && !fail; ++sweep) {
         if (tid == 0) s_rot = 0;
         __syncthreads();
-        for (int e = tid; e < nb; e += NT) { mod_prev[e] = mod_cur[e]; mod_cur[e] = 0; }
-        __syncthreads();
+        // order the columns by descending norm for this sweep (fewer sweeps in block-row-cyclic
+        // order); the staging buffer is free between sweeps and holds the sort keys
+        {
+            double* key = reinterpret_cast<double*>(smraw);
+            int* idx = reinterpret_cast<int*>(key + P2);
+            for (int c = warp; c < P2; c += NW) {
+                double sj = -1.0;
+                if (c < N) {
+                    const V* w = W + (long long)c * ld;
+                    sj = 0.0;
+                    for (int row = lane; row < R; row += 32)
+                        sj += (double)w[row].x * w[row].x + (double)w[row].y * w[row].y;
+                    sj = warp_sum(sj);
+                }
+                if (lane == 0) { key[c] = sj; idx[c] = c; }
+            }
+            __syncthreads();
+            bitonic_desc(key, idx, P2);
+            for (int e = tid; e < N; e += NT) {
+                perm[e] = idx[e];
+                cprev[e] = ccur[e];
+                ccur[e] = 0;
+            }
+            moved += (double)N / BW;
+            __syncthreads();
+        }
         int rot = 0;
         for (int I = 0; I < nb && !fail; ++I) {
-            const bool iflag = mod_prev[I] || mod_cur[I];
+            const bool iflag = blk_dirty(I);
             int jn = next_needed(I + 1, iflag);
             if (!iflag && jn >= nb) continue;  // every pair of block I is unchanged and orthogonal
-            if (tid == 0) { s_irot = 0; rc_stage<T>(ci, W, ld, rc, R, N, I, BW, &bars[0]); }
+            if (tid == 0) { s_irot = 0; rc_stage<T>(ci, W, ld, rc, R, N, I, BW, &bars[0], perm); }
             moved += 1.0;
             if (!wait(0)) { fail = true; break; }
             // inner pairs of block I: circle method, BW/2 pairs per round, G2 threads each
@@ -1650,11 +1707,11 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
                 xi[k] = row < R ? ci[warp * rc + row] : czero<V>();
             }
             __syncthreads();  // ci free for the next block I
-            if (jn < nb && tid == 0) rc_stage<T>(cj[0], W, ld, rc, R, N, jn, BW, &bars[1]);
+            if (jn < nb && tid == 0) rc_stage<T>(cj[0], W, ld, rc, R, N, jn, BW, &bars[1], perm);
             int b = 0;
             for (int J = jn; J < nb; J = jn, b ^= 1) {
                 jn = next_needed(J + 1, iflag);
-                if (jn < nb && tid == 0) rc_stage<T>(cj[b ^ 1], W, ld, rc, R, N, jn, BW, &bars[1 + (b ^ 1)]);
+                if (jn < nb && tid == 0) rc_stage<T>(cj[b ^ 1], W, ld, rc, R, N, jn, BW, &bars[1 + (b ^ 1)], perm);
                 if (tid == 0) s_jrot = 0;
                 if (!wait(1 + b)) { fail = true; break; }
                 pairs_checked += (double)BW * BW;
@@ -1708,10 +1765,10 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
                 // block J back to global memory when it changed; later bulk copies read it
                 if (s_jrot) {
                     moved += 1.0;
-                    if (tid == 0) mod_cur[J] = 1;
                     for (int c = warp; c < BW; c += NW) {
                         if (J * BW + c >= N) continue;
-                        V* dst = W + (long long)(J * BW + c) * ld;
+                        if (lane == 0) ccur[perm[J * BW + c]] = 1;
+                        V* dst = W + (long long)perm[J * BW + c] * ld;
                         const V* src = cb + c * rc;
                         for (int row = lane; row < R; row += 32) dst[row] = src[row];
                     }
@@ -1721,10 +1778,10 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
             }
             if (fail) break;
             const bool i_changed = s_irot != 0;
-            if (i_changed && tid == 0) mod_cur[I] = 1;
+            if (i_changed && vi && lane == 0) ccur[perm[I * BW + warp]] = 1;
             if (i_changed) moved += 1.0;
             if (vi && i_changed) {
-                V* dst = W + (long long)(I * BW + warp) * ld;
+                V* dst = W + (long long)perm[I * BW + warp] * ld;
 #pragma unroll
                 for (int k = 0; k < RPL; ++k) {
                     const int row = lane + 32 * k;
