@@ -78,6 +78,9 @@ def tune(problems, chi: int, precision: str = "c128", gates: int = 2, q0: int | 
     n = problems[0].n
     if q0 is None:
         q0 = 16 * min(32, n // 4)  # interior gate slots (saturated bonds for long chains)
+    ups = min(p.updates_per_step() for p in problems)
+    q0 = max(0, min(q0, ups - 1 - gates))
+    gates = min(gates, ups - 1 - q0)
     measured = {}
     for block, tc in candidates(precision):
         t0 = time.perf_counter()
