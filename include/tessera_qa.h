@@ -225,6 +225,9 @@ TESSERA_QA_API int tessera_qa_gnn_train_step(tessera_qa_gnn* g, const tessera_qa
                                              const float* target_knots, const float* target_spins, float lr,
                                              float lambda_knots, float lambda_spins, float* out_loss,
                                              float* out_grads, size_t grads_count);
+/* One Adam step with a gradient supplied by the caller (param_count floats), e.g. the average of
+ * the train_step gradients of several data-parallel ranks; the same update train_step applies. */
+TESSERA_QA_API int tessera_qa_gnn_apply_grads(tessera_qa_gnn* g, const float* grads, size_t count, float lr);
 /* Schedule prediction (the learned layer's inference): out_knots count x knots; out_bias (total
  * nodes, may be NULL) = 2 P(s_i = +1) - 1 in [-1, 1]. */
 TESSERA_QA_API int tessera_qa_schedule_predict(tessera_qa_gnn* g, const tessera_qa_problem* problems, size_t count,

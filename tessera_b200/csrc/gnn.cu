@@ -564,6 +564,11 @@ public:
         if (out_p) GN_CK(cudaMemcpyAsync(out_p, p, sizeof(float) * Nn, cudaMemcpyDeviceToHost, st));
         GN_CK(cudaStreamSynchronize(st));
     }
+    // an externally reduced gradient (data-parallel training) into the gradient buffer
+    void write_grads(const float* in) {
+        GN_CK(cudaStreamSynchronize(st));
+        GN_CK(cudaMemcpy(g, in, sizeof(float) * Ly.total, cudaMemcpyHostToDevice));
+    }
     void read_grads(float* out) {
         GN_CK(cudaStreamSynchronize(st));
         GN_CK(cudaMemcpy(out, g, sizeof(float) * Ly.total, cudaMemcpyDeviceToHost));
@@ -820,6 +825,17 @@ int tessera_qa_gnn_train_step(tessera_qa_gnn* g, const tessera_qa_problem* probl
             g->net->read_grads(out_grads);
         }
         if (lr > 0.f) g->net->adam(lr);
+        return 0;
+    });
+}
+
+int tessera_qa_gnn_apply_grads(tessera_qa_gnn* g, const float* grads, size_t count, float lr) {
+    return gn_guard([&]() -> int {
+        if (!g || !grads || count < g->net->Ly.total || !(lr > 0.f))
+            throw std::invalid_argument("gnn apply_grads: bad arguments");
+        g->net->write_grads(grads);
+        g->net->adam(lr);
+        GN_CK(cudaDeviceSynchronize());
         return 0;
     });
 }

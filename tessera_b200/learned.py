@@ -51,6 +51,8 @@ def _setup(L):
     L.tessera_qa_gnn_train_step.argtypes = [C.c_void_p, C.POINTER(_lib.Problem), C.c_size_t, fp, fp, C.c_float,
                                             C.c_float, C.c_float, fp, fp, C.c_size_t]
     L.tessera_qa_gnn_train_step.restype = C.c_int
+    L.tessera_qa_gnn_apply_grads.argtypes = [C.c_void_p, fp, C.c_size_t, C.c_float]
+    L.tessera_qa_gnn_apply_grads.restype = C.c_int
     L.tessera_qa_schedule_predict.argtypes = [C.c_void_p, C.POINTER(_lib.Problem), C.c_size_t, _lib.c_double_p,
                                               _lib.c_double_p]
     L.tessera_qa_schedule_predict.restype = C.c_int
@@ -133,6 +135,11 @@ class ScheduleGNN:
                                                   lambda_knots, lambda_spins, C.byref(loss),
                                                   _fptr(g) if g is not None else None, self.param_count))
         return float(loss.value), g
+
+    def apply_grads(self, grads, lr=1e-3):
+        """Adam step with a caller-supplied gradient (tessera_qa_gnn_apply_grads)."""
+        a = np.ascontiguousarray(grads, np.float32)
+        self._ck(self.L.tessera_qa_gnn_apply_grads(self._h, _fptr(a), a.size, lr))
 
     def predict(self, problems):
         """(knots (G, K), list of per-problem bias arrays in [-1, 1]) via tessera_qa_schedule_predict."""
@@ -245,6 +252,42 @@ def train(gnn: ScheduleGNN, problems, target_knots, ground_spins, epochs=200, ba
             loss, _ = gnn.train_step(ps, target_knots[sel], spin_targets([ground_spins[i] for i in sel]), lr=lr,
                                      lambda_spins=lambda_spins)
             losses.append(loss)
+    return losses
+
+
+def train_data_parallel(gnn, problems, target_knots, ground_spins, epochs=100, batch=32, lr=2e-3, seed=0,
+                        lambda_spins=0.2, group=None):
+    """Data-parallel training over torch.distributed ranks (one GPU each): every rank draws the same
+    mini-batch order, takes its contiguous share of each batch, computes loss and gradient with the
+    library's kernels, and the gradients are averaged (weighted by the share sizes) with one
+    all-reduce before the same Adam step on every rank, so the replicas stay identical.  Returns
+    the averaged loss per step."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    rng = np.random.Generator(np.random.PCG64(seed))
+    idx = np.arange(len(problems))
+    losses = []
+    for _ in range(epochs):
+        rng.shuffle(idx)
+        for s in range(0, len(idx), batch):
+            sel = idx[s:s + batch]
+            share = np.array_split(sel, world)[rank]
+            buf = torch.zeros(gnn.param_count + 2, dtype=torch.float64, device=dev)
+            if len(share):
+                ps = [problems[i] for i in share]
+                loss, g = gnn.train_step(ps, target_knots[share], spin_targets([ground_spins[i] for i in share]),
+                                         lr=0.0, lambda_spins=lambda_spins, want_grads=True)
+                w = float(len(share))
+                buf[:-2] = torch.from_numpy(g.astype(np.float64) * w)
+                buf[-2] = loss * w
+                buf[-1] = w
+            dist.all_reduce(buf, group=group)
+            tot = float(buf[-1])
+            gnn.apply_grads((buf[:-2] / tot).cpu().numpy(), lr=lr)
+            losses.append(float(buf[-2]) / tot)
     return losses
 
 

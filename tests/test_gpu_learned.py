@@ -102,3 +102,20 @@ def test_training_reduces_loss_and_beats_the_untrained_network():
     ev = learned.evaluate(net, test_p, cfg)
     assert ev["chosen_solved"] >= ev["plain_solved"]
     assert ev["chosen_mean_gap"] <= ev["plain_mean_gap"] + 1e-9
+
+
+def test_apply_grads_is_the_train_step_update():
+    """tessera_qa_gnn_apply_grads (the data-parallel path's optimizer step) applies exactly the Adam
+    update that train_step applies to its own gradient."""
+    probs = [instances.dense_er(n, 40 + n, T=1.0) for n in (6, 8, 9)]
+    rng = np.random.Generator(np.random.PCG64(2))
+    tk = np.sort(rng.random((len(probs), 16)), axis=1)
+    tk[:, 0], tk[:, -1] = 0.0, 1.0
+    ts = np.concatenate([rng.integers(0, 2, p.n).astype(np.float32) for p in probs])
+    a = learned.ScheduleGNN(seed=4, bf16=False)
+    b = learned.ScheduleGNN(seed=4, bf16=False)
+    for _ in range(2):
+        a.train_step(probs, tk, ts, lr=1e-2)
+        _, g = b.train_step(probs, tk, ts, lr=0.0, want_grads=True)
+        b.apply_grads(g, lr=1e-2)
+    assert np.array_equal(a.get_params(), b.get_params())

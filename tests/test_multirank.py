@@ -45,3 +45,70 @@ def test_two_gloo_ranks_shard_instances_and_take_max_time():
         flat = [i for v in allv for i in v]
         assert sorted(flat) == list(range(6))        # disjoint, complete
         assert ms == pytest.approx(15.0)              # slowest rank's time
+
+
+class _FakeNet:
+    """Stands in for ScheduleGNN on CPU: a parameter vector pulled towards a per-problem target
+    (the problem's n), mean squared loss over the problems of a step, plain gradient steps."""
+
+    def __init__(self, dim=5):
+        import numpy as np
+        self.theta = np.zeros(dim)
+        self.param_count = dim
+
+    def train_step(self, problems, tk, ts, lr=0.0, lambda_spins=0.2, want_grads=True):
+        import numpy as np
+        t = np.array([[float(p.n)] * self.param_count for p in problems])
+        d = self.theta[None, :] - t
+        return float(np.mean(np.sum(d * d, axis=1))), (2.0 * d.mean(axis=0)).astype(np.float32)
+
+    def apply_grads(self, g, lr=1e-3):
+        self.theta = self.theta - lr * g
+
+
+def _dp_rank(rank, world, port, q):
+    import numpy as np
+    import torch.distributed as dist
+
+    from tessera_b200 import instances, learned
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    probs = [instances.dense_er(n, 10 + n, T=1.0) for n in range(4, 15)]
+    net = _FakeNet()
+    losses = learned.train_data_parallel(net, probs, np.zeros((len(probs), 16)), [np.ones(p.n) for p in probs],
+                                         epochs=3, batch=4, lr=0.1, seed=5)
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((rank, net.theta.tolist(), losses))
+
+
+def test_data_parallel_training_matches_one_process():
+    """learned.train_data_parallel on two gloo ranks: the replicas stay identical and follow the
+    same trajectory as one process taking full-batch steps (the gradient all-reduce is weighted
+    by the share sizes, so uneven shares average correctly)."""
+    import numpy as np
+
+    from tessera_b200 import instances, learned
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_dp_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    out = sorted(q.get(timeout=180) for _ in ps)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert np.allclose(out[0][1], out[1][1], rtol=0, atol=0)
+    # serial reference: same batch order, full-batch mean gradient
+    probs = [instances.dense_er(n, 10 + n, T=1.0) for n in range(4, 15)]
+    net = _FakeNet()
+    rng = np.random.Generator(np.random.PCG64(5))
+    idx = np.arange(len(probs))
+    for _ in range(3):
+        rng.shuffle(idx)
+        for s in range(0, len(idx), 4):
+            _, g = net.train_step([probs[i] for i in idx[s:s + 4]], None, None)
+            net.apply_grads(g.astype(np.float64), lr=0.1)
+    assert np.allclose(out[0][1], net.theta, rtol=1e-6, atol=1e-6)
+    assert learned.spin_targets([np.ones(2)]).tolist() == [1.0, 1.0]
