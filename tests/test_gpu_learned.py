@@ -105,8 +105,9 @@ def test_training_reduces_loss_and_beats_the_untrained_network():
 
 
 def test_apply_grads_is_the_train_step_update():
-    """tessera_qa_gnn_apply_grads (the data-parallel path's optimizer step) applies exactly the Adam
-    update that train_step applies to its own gradient."""
+    """tessera_qa_gnn_apply_grads (the data-parallel path's optimizer step) applies the Adam update
+    that train_step applies to its own gradient.  The backward kernels sum with atomics, so two
+    networks' gradients differ in the last bits: parameters agree to 1e-5 relative."""
     probs = [instances.dense_er(n, 40 + n, T=1.0) for n in (6, 8, 9)]
     rng = np.random.Generator(np.random.PCG64(2))
     tk = np.sort(rng.random((len(probs), 16)), axis=1)
@@ -118,4 +119,6 @@ def test_apply_grads_is_the_train_step_update():
         a.train_step(probs, tk, ts, lr=1e-2)
         _, g = b.train_step(probs, tk, ts, lr=0.0, want_grads=True)
         b.apply_grads(g, lr=1e-2)
-    assert np.array_equal(a.get_params(), b.get_params())
+    pa, pb = a.get_params(), b.get_params()
+    assert np.allclose(pa, pb, rtol=1e-5, atol=1e-7)
+    assert np.max(np.abs(pa - learned.ScheduleGNN(seed=4, bf16=False).get_params())) > 1e-3  # it moved
