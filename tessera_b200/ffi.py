@@ -418,7 +418,7 @@ def sv_anneal(h, ei, ej, ew, sa, sb, dt=0.1, mode=0, bias=None, sc=None, want_st
 
 
 def anneal_batch(problems, dt=None, chi=None, precision="c128", zz_substeps=1, want_checkpoint=False,
-                 raise_on_status=True, skip_observables=False, jacobi_block=0, device=-1):
+                 raise_on_status=True, skip_observables=False, jacobi_block=0, device=-1, theta_tensor_cores=False):
     """tessera_qa_anneal_batch over a list of instances.Problem (each uses its own dt and chi unless
     overridden); returns a list of AnnealResult in the same order."""
     L = _lib.load()
@@ -434,7 +434,7 @@ def anneal_batch(problems, dt=None, chi=None, precision="c128", zz_substeps=1, w
         P_arr[b] = Pb
         cb, _ = config_struct(dt=dt if dt is not None else p.dt, chi=chi if chi is not None else p.chi,
                               precision=precision, zz_substeps=zz_substeps, jacobi_block=jacobi_block,
-                              device=device, skip_observables=skip_observables)
+                              device=device, skip_observables=skip_observables, theta_tensor_cores=theta_tensor_cores)
         C_arr[b] = cb
         n, steps = p.n, p.steps
         spins = np.zeros(n, np.int8)

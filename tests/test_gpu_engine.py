@@ -423,3 +423,16 @@ def test_mps_sampling_matches_state_probabilities():
     again, _ = s.sample(100, seed=7)
     assert np.array_equal(again, spins[:100])
     s.close()
+
+
+def test_precision_study_against_exact_state_vector():
+    """The three arithmetic modes against the FP64 state vector at exact chi (16 instances, n=12):
+    complex128 to rounding, complex64 (CUDA cores or split-TF32 tensor cores) to FP32 accuracy."""
+    from tessera_b200 import precision
+    r = precision.study(count=16)
+    assert r["c128"]["infidelity_max"] < 1e-10 and r["c128"]["energy_rel_err_max"] < 1e-9
+    for mode in ("c64", "c64_tensor_cores"):
+        assert r[mode]["infidelity_max"] < 1e-4, (mode, r[mode])
+        assert r[mode]["energy_rel_err_max"] < 1e-3, (mode, r[mode])
+        assert r[mode]["schmidt_dev_max"] < 1e-3, (mode, r[mode])
+    assert all(r[m]["status"] == [0] for m in ("c128", "c64", "c64_tensor_cores"))
