@@ -436,3 +436,28 @@ def test_precision_study_against_exact_state_vector():
         assert r[mode]["energy_rel_err_max"] < 1e-3, (mode, r[mode])
         assert r[mode]["schmidt_dev_max"] < 1e-3, (mode, r[mode])
     assert all(r[m]["status"] == [0] for m in ("c128", "c64", "c64_tensor_cores"))
+
+
+def test_ragged_three_regular_batch_with_mixed_chi():
+    """The batching workload's shape: random 3-regular graphs of uneven n (32..40) with bond caps
+    chi = 64 or 128 in one batched session (complex64, long-range edges through the swap network,
+    random saturated MPS).  Each instance's state after a window of gate slots, loaded into a
+    single-instance session, has the same <H> as the same slots run on that instance alone."""
+    probs = instances.batch_3_regular(count=6, T=0.2, dt=0.05, nmin=32, nmax=40)
+    assert len({p.chi for p in probs}) == 2 and len({p.n for p in probs}) > 1
+    sb = ffi.Session.batch(probs, precision="c64")
+    sb.randomize(17)
+    sb.run_gates(2, 10, 16)
+    rb = sb.sync()
+    assert rb.status == 0 and rb.two_site_updates == 6 * len(probs)
+    for b, p in enumerate(probs):
+        s1 = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=p.chi, precision="c64")
+        s1.randomize(17 + 7919 * b)
+        s1.run_gates(2, 10, 16)
+        assert s1.sync().status == 0
+        e_single = s1.observe().expected_energy
+        s1.load(sb.save_instance(b))
+        e_batch = s1.observe().expected_energy
+        s1.close()
+        assert e_batch == pytest.approx(e_single, rel=1e-3, abs=1e-4), (b, p.n, p.chi)
+    sb.close()
