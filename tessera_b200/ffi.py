@@ -288,7 +288,8 @@ class Session:
                                   precision=precision, **kw)
             cb.kernel_timing = 1 if kernel_timing else 0
             Carr[b] = cb
-        self.chi = chi
+        self._chis = [int(Carr[b].chi) for b in range(B)]
+        self.chi = chi if chi is not None else max(self._chis)
         self.n = problems[0].n
         self.count = B
         self._h = L.tessera_qa_session_create_batch(self._Parr, Carr, B)
@@ -356,7 +357,8 @@ class Session:
 
     def save_instance(self, index: int) -> bytes:
         """Checkpoint of instance `index` of a batched session (tessera_qa_session_save_instance)."""
-        nb = self._L.tessera_qa_checkpoint_bytes(self.n_of(index), self.chi)
+        chi = self._chis[index] if hasattr(self, "_chis") else self.chi
+        nb = self._L.tessera_qa_checkpoint_bytes(self.n_of(index), chi)
         buf = np.zeros(nb, np.uint8)
         self._ck(self._L.tessera_qa_session_save_instance(self._h, index, buf.ctypes.data, nb))
         return buf.tobytes()
