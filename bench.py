@@ -68,6 +68,9 @@ def parse():
     ap.add_argument("--solve-T", type=float, default=10.0, help="anneal time of the solves/s workload")
     ap.add_argument("--profile-run", action="store_true",
                     help="one untimed step only (for ncu); prints no bench line")
+    ap.add_argument("--profile-sv", action="store_true",
+                    help="one exact state-vector anneal, n=24 (a 256 MiB state), 4 steps (the tiled gate passes, "
+                         "for ncu); prints no bench line")
     ap.add_argument("--profile-anneal", action="store_true",
                     help="one batched anneal of 148 dense ER instances n=12, chi=32, T=0.3 (the small-bond resident "
                          "kernel, for ncu); prints no bench line")
@@ -322,6 +325,17 @@ def profile_anneal():
           f"{sorted(set(r.status for r in res))}, {res[0].device_ms:.1f} ms")
 
 
+def profile_sv():
+    from tessera_b200 import ffi, instances
+    p = instances.chain_range(n=24, dmax=2, seed=5, T=0.4, dt=0.1)
+    r = ffi.sv_anneal(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, mode=1)
+    # per step: 2 half steps x 4 tiled passes (read + write 16 B per amplitude), the ZZ phase
+    # (16 B read + 16 B write + 8 B diagonal) and the qubit-0 reduction (16 B read)
+    bytes_step = (2 * 4 * 32 + 40 + 16) * float(1 << 24)
+    print(f"profile sv: n=24, {p.steps} steps, {r.device_ms:.2f} ms, norm {r.norm2:.12f}, "
+          f"{bytes_step * p.steps / (r.device_ms / 1e3) / 1e9:.0f} GB/s algorithmic")
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -329,6 +343,9 @@ def main():
         return
     if args.profile_anneal:
         profile_anneal()
+        return
+    if args.profile_sv:
+        profile_sv()
         return
     import numpy as np
     import torch
