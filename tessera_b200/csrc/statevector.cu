@@ -14,7 +14,8 @@
 // Single-qubit gates are applied in tiles: a CTA loads the 2^(5+K) amplitudes that share all
 // bits outside {0..4} and K target qubits (the low five bits keep the loads coalesced), applies
 // the gates of every target in shared memory, and writes the tile back -- one HBM round trip per
-// pass instead of one per qubit.  Passes cover qubits 0..10, then six high qubits at a time.
+// pass instead of one per qubit.  Passes cover qubits 0..11, then the rest in even groups of at
+// most seven (n = 24: three passes per half step).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -38,16 +39,17 @@ void set_last_error(const std::string& msg);
     } while (0)
 
 constexpr int SV_LOW = 5;         // low bits always in a tile
-constexpr int SV_TGT = 6;         // target qubits per tile above the low bits
+constexpr int SV_TGT = 7;         // at most this many target qubits per tile above the low bits
 constexpr int SV_NT = 256;
 constexpr int SV_MAXN = 30;
 
 struct SvPass {
     int nt;            // tile bits (low + targets)
-    int pos[11];       // bit position in x of tile bit t
+    int nlow;          // tile bits 0..nlow-1 are x bits 0..nlow-1
+    int pos[12];       // bit position in x of tile bit t
     int ngate;         // gates applied in this pass
-    int gq[11];        // tile bit index of each gated qubit
-    int qubit[11];     // its qubit number (row of the gate table)
+    int gq[12];        // tile bit index of each gated qubit
+    int qubit[12];     // its qubit number (row of the gate table)
     int nrest;         // bits outside the tile
     int rpos[SV_MAXN]; // their positions in x, ascending
 };
@@ -106,9 +108,10 @@ __global__ void __launch_bounds__(SV_NT) k_sv_pass(double2* psi, SvPass ps, cons
     unsigned long long base = 0, r = blockIdx.x;
     for (int b = 0; b < ps.nrest; ++b, r >>= 1)
         if (r & 1ull) base |= 1ull << ps.rpos[b];
+    const int lowmask = (1 << ps.nlow) - 1;
     for (int t = threadIdx.x; t < T; t += SV_NT) {
-        unsigned long long x = base;
-        for (int b = 0; b < ps.nt; ++b)
+        unsigned long long x = base | (unsigned long long)(t & lowmask);
+        for (int b = ps.nlow; b < ps.nt; ++b)
             if ((t >> b) & 1) x |= 1ull << ps.pos[b];
         tile[t] = psi[x];
     }
@@ -129,8 +132,8 @@ __global__ void __launch_bounds__(SV_NT) k_sv_pass(double2* psi, SvPass ps, cons
         __syncthreads();
     }
     for (int t = threadIdx.x; t < T; t += SV_NT) {
-        unsigned long long x = base;
-        for (int b = 0; b < ps.nt; ++b)
+        unsigned long long x = base | (unsigned long long)(t & lowmask);
+        for (int b = ps.nlow; b < ps.nt; ++b)
             if ((t >> b) & 1) x |= 1ull << ps.pos[b];
         psi[x] = tile[t];
     }
@@ -239,25 +242,39 @@ __global__ void k_sv_final(const double2* psi, const double* dfull, unsigned lon
     }
 }
 
+// Passes of one half step: the first gates the low bits and the next SV_TGT qubits; the rest
+// are spread evenly over as few passes as hold at most SV_TGT targets each (no small last pass).
 static std::vector<SvPass> plan_passes(int n) {
     std::vector<SvPass> out;
     const int low = n < SV_LOW ? n : SV_LOW;
-    int next = 0;  // first qubit not yet gated
-    while (next < n) {
+    std::vector<std::vector<int>> groups;
+    std::vector<int> first;
+    for (int q = low; q < n && (int)first.size() < SV_TGT; ++q) first.push_back(q);
+    groups.push_back(first);
+    const int start = low + (int)first.size(), rem = n - start;
+    if (rem > 0) {
+        const int np = (rem + SV_TGT - 1) / SV_TGT;
+        int q = start;
+        for (int k = 0; k < np; ++k) {
+            const int cnt = rem / np + (k < rem % np ? 1 : 0);
+            std::vector<int> g;
+            for (int c = 0; c < cnt; ++c) g.push_back(q++);
+            groups.push_back(g);
+        }
+    }
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
         SvPass p{};
         p.nt = 0;
-        // low bits always in the tile
-        for (int b = 0; b < low; ++b) p.pos[p.nt++] = b;
+        p.nlow = low;
+        for (int b = 0; b < low; ++b) p.pos[p.nt++] = b;  // low bits always in the tile
         p.ngate = 0;
-        if (next < low) {
+        if (gi == 0)
             for (int b = 0; b < low; ++b) { p.gq[p.ngate] = b; p.qubit[p.ngate] = b; ++p.ngate; }
-            next = low;
-        }
-        for (int c = 0; c < SV_TGT && next < n; ++c, ++next) {
+        for (int q : groups[gi]) {
             p.gq[p.ngate] = p.nt;
-            p.qubit[p.ngate] = next;
+            p.qubit[p.ngate] = q;
             ++p.ngate;
-            p.pos[p.nt++] = next;
+            p.pos[p.nt++] = q;
         }
         p.nrest = 0;
         for (int b = 0; b < n; ++b) {
