@@ -329,11 +329,12 @@ def profile_sv():
     from tessera_b200 import ffi, instances
     p = instances.chain_range(n=24, dmax=2, seed=5, T=0.4, dt=0.1)
     r = ffi.sv_anneal(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, mode=1)
-    # per step: 2 half steps x 3 tiled passes (read + write 16 B per amplitude), the ZZ phase
-    # (16 B read + 16 B write + 8 B diagonal) and the qubit-0 reduction (16 B read)
-    bytes_step = (2 * 3 * 32 + 40 + 16) * float(1 << 24)
+    # steps + 1 sweeps of 3 tiled passes (read + write 16 B per amplitude each), the ZZ diagonal
+    # read once per step (8 B, fused into a sweep), the diagonals' set-up (32 B written) and the
+    # readout (24 B read)
+    bytes_run = ((p.steps + 1) * 3 * 32 + p.steps * 8 + 32 + 24) * float(1 << 24)
     print(f"profile sv: n=24, {p.steps} steps, {r.device_ms:.2f} ms, norm {r.norm2:.12f}, "
-          f"{bytes_step * p.steps / (r.device_ms / 1e3) / 1e9:.0f} GB/s algorithmic")
+          f"{bytes_run / (r.device_ms / 1e3) / 1e9:.0f} GB/s algorithmic")
 
 
 def main():

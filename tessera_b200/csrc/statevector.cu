@@ -15,7 +15,12 @@
 // bits outside {0..4} and K target qubits (the low five bits keep the loads coalesced), applies
 // the gates of every target in shared memory, and writes the tile back -- one HBM round trip per
 // pass instead of one per qubit.  Passes cover qubits 0..11, then the rest in even groups of at
-// most seven (n = 24: three passes per half step).
+// most seven (n = 24: three passes per half step).  The diagonal phases ride on the first pass's
+// load and the last pass's store, and the last pass of a step also sums the qubit-0 reduced
+// density matrix over its tile, so a mode-0 step is exactly one sweep of passes (three round
+// trips of psi at n = 24).  In mode 1 the closing single-qubit half step of one step and the
+// opening one of the next are merged into one gate per qubit, so that mode too costs one sweep
+// per step (plus one).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -76,13 +81,10 @@ __global__ void k_sv_diag(const double* h, const int* ei, const int* ej, const d
     }
 }
 
-// 2x2 gate of every qubit for step k (row-major u00 u01 u10 u11).
-__global__ void k_sv_gates(const double* h, const double* sa, const double* sb, const double* bias, const double* sc,
-                           int n, int k, double dt, int mode, double2* gates) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+// 2x2 single-qubit gate of qubit i at step k (row-major u00 u01 u10 u11).
+__device__ void sv_gate(const double* h, const double* sa, const double* sb, const double* bias, const double* sc,
+                        int i, int k, double dt, int mode, double2 g[4]) {
     const double A = sa[k], B = sb[k];
-    double2* g = gates + 4 * i;
     if (mode == 0) {  // exp(+i A dt X)
         const double c = cos(A * dt), s = sin(A * dt);
         g[0] = make_double2(c, 0.0); g[1] = make_double2(0.0, s);
@@ -100,9 +102,46 @@ __global__ void k_sv_gates(const double* h, const double* sa, const double* sb, 
     }
 }
 
-// One tiled pass of single-qubit gates.
-__global__ void __launch_bounds__(SV_NT) k_sv_pass(double2* psi, SvPass ps, const double2* gates) {
+// Gate of every qubit for step k, or, with k2 >= 0, the product G(k2) G(k) (G(k) applied first).
+__global__ void k_sv_gates(const double* h, const double* sa, const double* sb, const double* bias, const double* sc,
+                           int n, int k, int k2, double dt, int mode, double2* gates) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double2 g[4];
+    sv_gate(h, sa, sb, bias, sc, i, k, dt, mode, g);
+    if (k2 >= 0) {
+        double2 f[4];
+        sv_gate(h, sa, sb, bias, sc, i, k2, dt, mode, f);
+        for (int r = 0; r < 2; ++r)
+            for (int c = 0; c < 2; ++c) {
+                const double2 x = zmul(f[2 * r], g[c]), y = zmul(f[2 * r + 1], g[2 + c]);
+                gates[4 * i + 2 * r + c] = make_double2(x.x + y.x, x.y + y.y);
+            }
+    } else {
+        for (int q = 0; q < 4; ++q) gates[4 * i + q] = g[q];
+    }
+}
+
+// Diagonal phase fused into a pass: psi[x] *= exp(-i scale d[x]).
+struct SvPhase {
+    const double* d;  // NULL: none
+    double scale;
+};
+
+__device__ __forceinline__ double2 sv_phase(double2 v, const SvPhase& ph, unsigned long long x) {
+    double sn, cs;
+    sincos(-ph.scale * ph.d[x], &sn, &cs);
+    return zmul(v, make_double2(cs, sn));
+}
+
+// One tiled pass of single-qubit gates, with an optional diagonal phase applied on load (pre)
+// and before the store (post), and optional partial sums of the qubit-0 reduced density matrix
+// (r00, r11, Re r01, Im r01 per CTA into rho) of the gated tile: after the post phase, or
+// before it when rho_first is set.
+__global__ void __launch_bounds__(SV_NT) k_sv_pass(double2* psi, SvPass ps, const double2* gates, SvPhase pre,
+                                                   SvPhase post, double* rho, int rho_first) {
     extern __shared__ double2 tile[];
+    __shared__ double red[4][SV_NT / 32];
     const int T = 1 << ps.nt;
     // base index of this CTA: blockIdx spread over the rest bits
     unsigned long long base = 0, r = blockIdx.x;
@@ -113,7 +152,8 @@ __global__ void __launch_bounds__(SV_NT) k_sv_pass(double2* psi, SvPass ps, cons
         unsigned long long x = base | (unsigned long long)(t & lowmask);
         for (int b = ps.nlow; b < ps.nt; ++b)
             if ((t >> b) & 1) x |= 1ull << ps.pos[b];
-        tile[t] = psi[x];
+        const double2 v = psi[x];
+        tile[t] = pre.d ? sv_phase(v, pre, x) : v;
     }
     __syncthreads();
     for (int gI = 0; gI < ps.ngate; ++gI) {
@@ -131,55 +171,57 @@ __global__ void __launch_bounds__(SV_NT) k_sv_pass(double2* psi, SvPass ps, cons
         }
         __syncthreads();
     }
+    // the post phase goes into the tile first only when the reduction must see it
+    const bool post_in_tile = post.d && rho && !rho_first;
+    if (post_in_tile) {
+        for (int t = threadIdx.x; t < T; t += SV_NT) {
+            unsigned long long x = base | (unsigned long long)(t & lowmask);
+            for (int b = ps.nlow; b < ps.nt; ++b)
+                if ((t >> b) & 1) x |= 1ull << ps.pos[b];
+            tile[t] = sv_phase(tile[t], post, x);
+        }
+        __syncthreads();
+    }
+    if (rho) {  // tile bit 0 is x bit 0: pairs (2y, 2y + 1) differ in qubit 0 only
+        double a = 0, bb = 0, cr = 0, ci = 0;
+        for (int y = threadIdx.x; y < T / 2; y += SV_NT) {
+            const double2 u = tile[2 * y], v = tile[2 * y + 1];
+            a += u.x * u.x + u.y * u.y;
+            bb += v.x * v.x + v.y * v.y;
+            cr += u.x * v.x + u.y * v.y;  // u conj(v)
+            ci += u.y * v.x - u.x * v.y;
+        }
+        a = warp_sum(a); bb = warp_sum(bb); cr = warp_sum(cr); ci = warp_sum(ci);
+        const int w = threadIdx.x >> 5;
+        if ((threadIdx.x & 31) == 0) { red[0][w] = a; red[1][w] = bb; red[2][w] = cr; red[3][w] = ci; }
+        __syncthreads();
+        if (threadIdx.x < 4) {
+            double sum = 0;
+            for (int q = 0; q < SV_NT / 32; ++q) sum += red[threadIdx.x][q];
+            rho[4 * (size_t)blockIdx.x + threadIdx.x] = sum;
+        }
+    }
+    const bool post_on_store = post.d && !post_in_tile;
     for (int t = threadIdx.x; t < T; t += SV_NT) {
         unsigned long long x = base | (unsigned long long)(t & lowmask);
         for (int b = ps.nlow; b < ps.nt; ++b)
             if ((t >> b) & 1) x |= 1ull << ps.pos[b];
-        psi[x] = tile[t];
-    }
-}
-
-// psi[x] *= exp(-i scale d[x])
-__global__ void k_sv_phase(double2* psi, const double* d, double scale_k, const double* sb, int k, double factor,
-                           unsigned long long dim) {
-    const double scale = factor * sb[k] * scale_k;
-    for (unsigned long long x = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; x < dim;
-         x += (unsigned long long)gridDim.x * blockDim.x) {
-        double s, c;
-        sincos(-scale * d[x], &s, &c);
-        psi[x] = zmul(psi[x], make_double2(c, s));
-    }
-}
-
-// partial sums for the qubit-0 reduced density matrix: r00, r11, Re r01, Im r01
-__global__ void k_sv_rho0(const double2* psi, unsigned long long half, double* part) {
-    __shared__ double red[4][SV_NT / 32];
-    double a = 0, b = 0, cr = 0, ci = 0;
-    for (unsigned long long y = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; y < half;
-         y += (unsigned long long)gridDim.x * blockDim.x) {
-        const double2 u = psi[2 * y], v = psi[2 * y + 1];
-        a += u.x * u.x + u.y * u.y;
-        b += v.x * v.x + v.y * v.y;
-        cr += u.x * v.x + u.y * v.y;  // u conj(v)
-        ci += u.y * v.x - u.x * v.y;
-    }
-    a = warp_sum(a); b = warp_sum(b); cr = warp_sum(cr); ci = warp_sum(ci);
-    const int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) { red[0][w] = a; red[1][w] = b; red[2][w] = cr; red[3][w] = ci; }
-    __syncthreads();
-    if (threadIdx.x < 4) {
-        double s = 0;
-        for (int k = 0; k < SV_NT / 32; ++k) s += red[threadIdx.x][k];
-        part[4 * blockIdx.x + threadIdx.x] = s;
+        psi[x] = post_on_store ? sv_phase(tile[t], post, x) : tile[t];
     }
 }
 
 __global__ void k_sv_entropy(const double* part, int nblk, double* out, int k) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    __shared__ double red[4][SV_NT / 32];
+    double r[4] = {0, 0, 0, 0};
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+        for (int q = 0; q < 4; ++q) r[q] += part[4 * (size_t)b + q];
+    for (int q = 0; q < 4; ++q) r[q] = warp_sum(r[q]);
+    if ((threadIdx.x & 31) == 0)
+        for (int q = 0; q < 4; ++q) red[q][threadIdx.x >> 5] = r[q];
+    __syncthreads();
+    if (threadIdx.x != 0) return;
     double r00 = 0, r11 = 0, rr = 0, ri = 0;
-    for (int b = 0; b < nblk; ++b) {
-        r00 += part[4 * b]; r11 += part[4 * b + 1]; rr += part[4 * b + 2]; ri += part[4 * b + 3];
-    }
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { r00 += red[0][w]; r11 += red[1][w]; rr += red[2][w]; ri += red[3][w]; }
     const double tot = r00 + r11;
     double S = 0.0;
     if (tot > 0) {
@@ -329,7 +371,10 @@ extern "C" int tessera_qa_sv_anneal(const tessera_qa_problem* P, double dt, int 
         const size_t o_j = o_i + al(4 * (m + 1)), o_sa = o_j + al(4 * (m + 1)), o_sb = o_sa + al(8 * steps);
         const size_t o_bias = o_sb + al(8 * steps), o_sc = o_bias + al(8 * n), o_g = o_sc + al(8 * steps);
         const size_t o_part = o_g + al(64 * n), o_ent = o_part + al(8 * (size_t)grid * (3 + SV_MAXN));
-        const size_t o_bx = o_ent + al(8 * steps), total = o_bx + al(8 * (size_t)grid);
+        const std::vector<SvPass> passes = plan_passes(n);
+        const size_t rho_blocks = 1ull << passes.back().nrest;  // qubit-0 partials: one set per last-pass CTA
+        const size_t o_bx = o_ent + al(8 * steps), o_rho = o_bx + al(8 * (size_t)grid);
+        const size_t total = o_rho + al(32 * rho_blocks);
         SV_CK(cudaMalloc(&arena, total));
         auto at = [&](size_t o) { return arena + o; };
         double2* psi = (double2*)at(o_psi);
@@ -339,6 +384,7 @@ extern "C" int tessera_qa_sv_anneal(const tessera_qa_problem* P, double dt, int 
         double2* dg = (double2*)at(o_g);
         double *part = (double*)at(o_part), *dent = (double*)at(o_ent);
         unsigned long long* dbx = (unsigned long long*)at(o_bx);
+        double* drho = (double*)at(o_rho);
         cudaError_t err = cudaSuccess;
         auto cp = [&](void* d, const void* h, size_t bytes) {
             if (err == cudaSuccess && bytes) err = cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st);
@@ -356,39 +402,53 @@ extern "C" int tessera_qa_sv_anneal(const tessera_qa_problem* P, double dt, int 
         cudaEvent_t e0, e1;
         if (err == cudaSuccess) err = cudaEventCreate(&e0);
         if (err == cudaSuccess) err = cudaEventCreate(&e1);
-        const std::vector<SvPass> passes = plan_passes(n);
         int maxnt = 0;
         for (const SvPass& p : passes) maxnt = p.nt > maxnt ? p.nt : maxnt;
         const size_t tile_bytes = sizeof(double2) << maxnt;
         if (err == cudaSuccess && tile_bytes > 48 * 1024)
             err = cudaFuncSetAttribute(k_sv_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes);
-        const unsigned long long half = dim / 2;
-        const int rgrid = (int)std::min<unsigned long long>((half + SV_NT - 1) / SV_NT, (unsigned long long)grid);
         if (err == cudaSuccess) err = cudaMemsetAsync(dent, 0, 8 * (size_t)steps, st);  // n = 1: no entanglement
         if (err == cudaSuccess) {
             cudaEventRecord(e0, st);
             k_sv_diag<<<grid, SV_NT, 0, st>>>(dh, di, dj, dw, n, m, dim, df, dz, psi);
-            auto gates_pass = [&](int k) {
-                k_sv_gates<<<(n + 63) / 64, 64, 0, st>>>(dh, dsa, dsb, P->bias ? dbias : nullptr, dsc, n, k, dt, mode,
-                                                        dg);
-                for (const SvPass& p : passes) {
+            const SvPhase none{nullptr, 0.0};
+            const double* hsb = P->schedule_b;
+            auto gates = [&](int k, int k2) {
+                k_sv_gates<<<(n + 63) / 64, 64, 0, st>>>(dh, dsa, dsb, P->bias ? dbias : nullptr, dsc, n, k, k2, dt,
+                                                        mode, dg);
+            };
+            // One sweep of the gate passes; `pre` rides on the first pass's load, `post` and the
+            // qubit-0 partial sums on the last pass.
+            auto sweep = [&](SvPhase pre, SvPhase post, double* rho, int rho_first) {
+                for (size_t i = 0; i < passes.size(); ++i) {
+                    const SvPass& p = passes[i];
+                    const bool last = i + 1 == passes.size();
                     const unsigned long long blocks = 1ull << p.nrest;
-                    k_sv_pass<<<(unsigned)blocks, SV_NT, sizeof(double2) << p.nt, st>>>(psi, p, dg);
+                    k_sv_pass<<<(unsigned)blocks, SV_NT, sizeof(double2) << p.nt, st>>>(
+                        psi, p, dg, i == 0 ? pre : none, last ? post : none, last ? rho : nullptr, rho_first);
                 }
             };
-            for (int k = 0; k < steps; ++k) {
-                if (mode == 0) {
-                    k_sv_phase<<<grid, SV_NT, 0, st>>>(psi, df, dt, dsb, k, 0.5, dim);
-                    gates_pass(k);
-                    k_sv_phase<<<grid, SV_NT, 0, st>>>(psi, df, dt, dsb, k, 0.5, dim);
-                } else {
-                    gates_pass(k);
-                    k_sv_phase<<<grid, SV_NT, 0, st>>>(psi, dz, dt, dsb, k, 1.0, dim);
-                    gates_pass(k);
+            double* rho = n >= 2 ? drho : nullptr;
+            if (mode == 0) {  // P X P per step: one sweep, both phases fused into it
+                for (int k = 0; k < steps; ++k) {
+                    const SvPhase ph{df, 0.5 * hsb[k] * dt};
+                    gates(k, -1);
+                    sweep(ph, ph, rho, 0);
+                    if (rho) k_sv_entropy<<<1, SV_NT, 0, st>>>(rho, (int)rho_blocks, dent, k);
                 }
-                if (n >= 2) {
-                    k_sv_rho0<<<rgrid, SV_NT, 0, st>>>(psi, half, part);
-                    k_sv_entropy<<<1, 32, 0, st>>>(part, rgrid, dent, k);
+            } else {
+                // G(k) Z(k) G(k) per step.  The closing half step of step k and the opening one of
+                // step k+1 are single-qubit gates on every qubit, so they run as one sweep of
+                // the products G(k+1) G(k).  The qubit-0 entropy of step k is read from that
+                // sweep before the next ZZ phase: G(k+1) is a product of one-qubit unitaries,
+                // which leaves the Schmidt spectrum across the qubit-0 cut unchanged.
+                gates(0, -1);
+                sweep(none, SvPhase{dz, 1.0 * hsb[0] * dt}, nullptr, 0);
+                for (int k = 0; k < steps; ++k) {
+                    const bool more = k + 1 < steps;
+                    gates(k, more ? k + 1 : -1);
+                    sweep(none, more ? SvPhase{dz, 1.0 * hsb[k + 1] * dt} : none, rho, 1);
+                    if (rho) k_sv_entropy<<<1, SV_NT, 0, st>>>(rho, (int)rho_blocks, dent, k);
                 }
             }
             k_sv_final<<<grid, SV_NT, 0, st>>>(psi, df, dim, n, part, dbx);
