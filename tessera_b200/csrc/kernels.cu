@@ -303,10 +303,14 @@ __device__ __forceinline__ bool jacobi_rotation(const double v0, const double v1
     er = (T)(v2 * rg);
     ei = (T)(v3 * rg);
     if constexpr (sizeof(T) == 8) {
-        const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-        const double cs = rsqrt(1.0 + t * t);
-        c = cs;
-        s = cs * t;
+        // t = sgn(zeta) / u with u = |zeta| + sqrt(1 + zeta^2) = (|d| + sqrt(d^2 + 4 g2)) / (2 |gamma|),
+        // d = v1 - v0; then c = 1 / sqrt(1 + t^2) = u w and s = c t = sgn(zeta) w for
+        // w = 1 / sqrt(u^2 + 1).  No division, and the square root runs beside rsqrt(g2).
+        const double d = v1 - v0;
+        const double u = 0.5 * rg * (fabs(d) + sqrt(fma(d, d, 4.0 * g2)));
+        const double w = rsqrt(fma(u, u, 1.0));
+        c = u * w;
+        s = zeta >= 0 ? w : -w;
     } else {
         const float z = (float)zeta, az = fabsf(z);
         // for |zeta| >= 1e18 1 + zeta^2 overflows float; t = 1/(2 zeta) to float precision there
