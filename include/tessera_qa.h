@@ -153,7 +153,11 @@ TESSERA_QA_API size_t tessera_qa_checkpoint_bytes(size_t n, size_t chi);
 /* Thin SVD of one rows x cols complex128 matrix (row-major, interleaved re/im) through the
  * engine's one-sided Jacobi kernel: s (min(rows,cols), descending), u (rows x k) and vh
  * (k x cols), both row-major interleaved; u / vh may be NULL.  The counterpart of the
- * reference's tessera::svd (cuda/src/linalg.cpp:107-172). */
+ * reference's tessera::svd (cuda/src/linalg.cpp:107-172).  rows, cols <= 2048.  Singular
+ * values under the noise floor 8 sqrt(rows) ulps of ||A||_F are not resolved (their columns
+ * are frozen).  From about 1024 columns, a column whose norm dips under that floor during the
+ * sweeps stays frozen: a few values within ~4x of the floor can come back at it, and the u / vh
+ * columns of frozen values are then not orthogonal to the rest. */
 TESSERA_QA_API int tessera_qa_svd(const double* a, size_t rows, size_t cols, double* s, double* u, double* vh);
 
 /* Allocation-free SVD, for callers that cannot call cudaMalloc (their device memory belongs to
