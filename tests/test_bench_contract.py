@@ -1,0 +1,54 @@
+"""The JSON line of `bench.py --impl reference` on CPU: its keys, units and the extrapolation.
+
+The reference's own SVD sample (about 20 s per step on 16 threads) is replaced by a stub that
+returns fixed wall times, so only the line's assembly is under test: rank 0 alone prints one
+line; other ranks print nothing; value = threads / (t256 * 2^p) with p = log2(t256 / t128).
+"""
+import io
+import json
+import math
+import sys
+from contextlib import redirect_stdout
+
+import pytest
+
+import bench
+
+
+def _run(monkeypatch, argv, rank="0"):
+    from oracle import oracle as orc
+    monkeypatch.setattr(sys, "argv", ["bench.py"] + argv)
+    monkeypatch.setenv("RANK", rank)
+    monkeypatch.setattr(orc.Reference, "available", staticmethod(lambda: True))
+    times = {128: 0.05, 256: 0.8}
+    monkeypatch.setattr(bench, "ref_svd_sample", lambda m, threads, seed=0: times[m])
+    out = io.StringIO()
+    with redirect_stdout(out):
+        bench.run_reference(bench.parse())
+    return out.getvalue()
+
+
+def test_reference_line_keys_and_value(monkeypatch):
+    text = _run(monkeypatch, ["--impl", "reference", "--steps", "2", "--warmup", "1"])
+    lines = [l for l in text.splitlines() if l.strip()]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    assert d["metric"] == bench.METRIC and d["unit"] == bench.UNIT
+    assert d["steps"] == 2 and d["warmup"] == 1 and d["n_gpus"] == 1
+    assert d["higher_is_better"] is True and d["vs_baseline"] is None
+    p = math.log2(0.8 / 0.05)
+    threads = d["cpu_baseline"]["cores"]
+    assert threads >= 1
+    assert d["value"] == pytest.approx(threads / (0.8 * 2.0 ** p))
+    assert d["ms_per_step"] == pytest.approx(800.0)
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["value"] == d["value"] and cb["unit"] == bench.UNIT
+    assert "extrapolated" in cb["sample"]
+    e = d["e2e"]
+    assert e["value"] == d["value"] and e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
+    assert d["config"]["chi"] == 256 and d["config"]["updates_per_trotter_step"] == 1998
+
+
+def test_reference_line_only_on_rank_zero(monkeypatch):
+    assert _run(monkeypatch, ["--impl", "reference", "--steps", "1", "--warmup", "0"], rank="1") == ""
