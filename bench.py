@@ -99,6 +99,14 @@ def max_over_ranks(ms: float, world: int, device: str = "cuda") -> float:
     return float(t.item())
 
 
+def job_status(status: int, world: int, device: str = "cuda") -> int:
+    """Nonzero on every rank when any rank's run reported status bits (the largest value), so
+    all ranks stop together instead of some waiting at the next collective."""
+    if world <= 1:
+        return int(status)
+    return int(max_over_ranks(float(status), world, device=device))
+
+
 def fp64_peak_tflops() -> float:
     """FP64 peak of this GPU as cuBLAS reaches it: best of 5 DGEMMs of 4096^3 (CUDA events)."""
     import torch
@@ -422,8 +430,9 @@ def main():
     ms_max = max_over_ranks(ms, world)
     updates = r1.two_site_updates - r0.two_site_updates
     assert updates == B * G * args.steps, (updates, B, G)
-    if r1.status:
-        raise RuntimeError(f"engine status bits {r1.status} during the timed steps")
+    st = job_status(r1.status, world)
+    if st:
+        raise RuntimeError(f"engine status bits {st} during the timed steps (largest over ranks)")
     value = updates * world / (ms_max / 1e3)
     svd_n = r1.svd_launches - r0.svd_launches
     svd_ms = r1.svd_ms - r0.svd_ms
@@ -479,15 +488,21 @@ def main():
             pinned.append(cp)
         h2d = sum(q.h.nbytes + q.ew.nbytes + 2 * q.ei.nbytes + q.sa.nbytes + q.sb.nbytes for q in pinned)
         walls = []
+        e2e_status = 0
         for k in range(2):  # one untimed, one timed
             q0, q1 = window(args.warmup + args.steps + k)
             torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
             t0 = time.perf_counter()
             rr = sess.run_host(pinned, MID_STEP, q0, q1)
             walls.append(time.perf_counter() - t0)
-            if rr.status:
-                raise RuntimeError(f"engine status bits {rr.status} in the e2e step")
-        e2e = {"value": B * G * world / walls[-1], "unit": UNIT, "h2d_bytes_per_step": h2d,
+            e2e_status |= rr.status
+        st = job_status(e2e_status, world)
+        if st:
+            raise RuntimeError(f"engine status bits {st} in the e2e step (largest over ranks)")
+        wall = max_over_ranks(1e3 * walls[-1], world) / 1e3  # the slowest rank's call
+        e2e = {"value": B * G * world / wall, "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": 128 * B,
                "api": "tessera_qa_session_run_host (h, J, schedule of every instance from pinned host memory -> "
                       f"{G} gate slots -> run statistics to host)"}

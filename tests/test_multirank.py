@@ -1,5 +1,6 @@
 """The multi-rank plumbing of bench.py on CPU: two gloo ranks (127.0.0.1) take disjoint instance
-shards, agree on the job's step time as the max over ranks, and no rank exchanges instance data."""
+shards, agree on the job's step time as the max over ranks, learn of a bad run status on any
+rank, and no rank exchanges instance data."""
 import os
 import socket
 
@@ -25,9 +26,12 @@ def _rank(rank, world, port, q):
     allv = [None] * world
     dist.all_gather_object(allv, mine)
     ms = bench.max_over_ranks(10.0 + 5.0 * rank, world, device="cpu")
+    # a status set on rank 1 alone reaches rank 0 too; a clean job stays clean everywhere
+    st_bad = bench.job_status(4 if rank == 1 else 0, world, device="cpu")
+    st_ok = bench.job_status(0, world, device="cpu")
     dist.barrier()
     dist.destroy_process_group()
-    q.put((rank, allv, ms))
+    q.put((rank, allv, ms, st_bad, st_ok))
 
 
 def test_two_gloo_ranks_shard_instances_and_take_max_time():
@@ -41,10 +45,11 @@ def test_two_gloo_ranks_shard_instances_and_take_max_time():
     for p in ps:
         p.join(timeout=60)
         assert p.exitcode == 0
-    for rank, allv, ms in out:
+    for rank, allv, ms, st_bad, st_ok in out:
         flat = [i for v in allv for i in v]
         assert sorted(flat) == list(range(6))        # disjoint, complete
         assert ms == pytest.approx(15.0)              # slowest rank's time
+        assert st_bad == 4 and st_ok == 0            # every rank stops together
 
 
 class _FakeNet:
