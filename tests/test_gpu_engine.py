@@ -212,6 +212,22 @@ def test_complex64_mode_error_is_bounded(oracle):
     assert r64.expected_energy == pytest.approx(sv.expected_energy, rel=1e-4)
 
 
+def test_jacobi_sweep_cap_reports_not_converged():
+    """The give-up path: with the sweep cap forced to 1 the Jacobi cannot converge, the call
+    returns TESSERA_QA_ESTATUS with status bit 1 and still fills the result; the default cap
+    converges on the same input."""
+    from tessera_b200 import _lib
+    p = instances.chain_range(n=8, dmax=2, seed=9, T=1.0, dt=0.1, chi=8, dist="normal", hzero=False)
+    args = (p.h, p.ei, p.ej, p.ew, p.sa, p.sb)
+    with pytest.raises(_lib.EngineError) as err:
+        ffi.anneal(*args, dt=p.dt, chi=8, jacobi_max_sweeps=1)
+    assert err.value.code == _lib.ESTATUS
+    r = ffi.anneal(*args, dt=p.dt, chi=8, jacobi_max_sweeps=1, raise_on_status=False)
+    assert r.status & 1 and r.max_sweeps == 1 and r.two_site_updates > 0
+    ok = ffi.anneal(*args, dt=p.dt, chi=8)
+    assert ok.status == 0 and 1 < ok.max_sweeps < 60
+
+
 def test_checkpoint_resume_equals_straight_run():
     p = instances.chain_range(n=12, dmax=2, seed=5, T=3.0, dt=0.05, chi=8, dist="normal", hzero=False)
     full = ffi.anneal(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=8)
