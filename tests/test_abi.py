@@ -109,3 +109,49 @@ def test_checkpoint_decoder_roundtrip():
     psi = ffi.sites_to_dense(sites)
     ref = np.array([(a[0, s0] @ b[:, s1, 0]) for s1 in range(2) for s0 in range(2)])
     assert np.allclose(psi, ref)
+
+
+@pytest.mark.parametrize("case", ["n31", "steps1", "bad_dt", "bad_mode", "bias_mode0", "edge_oob", "nan_h"])
+def test_state_vector_rejects_invalid_input_without_a_gpu(case):
+    """tessera_qa_sv_anneal validates before its first CUDA call: EINVAL and a message."""
+    n = 31 if case == "n31" else 3
+    h = np.full(n, 0.1)
+    ei, ej, ew = np.array([0, 1]), np.array([1, 2]), np.array([0.5, -0.5])
+    steps = 1 if case == "steps1" else 5
+    sa, sb = np.linspace(1, 0, steps), np.linspace(0, 1, steps)
+    kw = dict(dt=0.1, mode=0)
+    if case == "bad_dt":
+        kw["dt"] = 0.0
+    elif case == "bad_mode":
+        kw["mode"] = 2
+    elif case == "bias_mode0":
+        kw.update(bias=np.ones(n), sc=np.ones(steps))
+    elif case == "edge_oob":
+        ej = np.array([1, 3])
+    elif case == "nan_h":
+        h[1] = np.nan
+    with pytest.raises(_lib.EngineError) as e:
+        ffi.sv_anneal(h, ei, ej, ew, sa, sb, **kw)
+    assert e.value.code == _lib.EINVAL
+    assert len(_lib.last_error()) > 0
+
+
+@pytest.mark.parametrize("shape", [(0, 4), (4, 0), (2049, 4), (4, 2049)])
+def test_svd_rejects_out_of_range_shapes_without_a_gpu(shape):
+    L = _lib.load()
+    r, c = shape
+    a = np.zeros(2 * max(r * c, 1))
+    s = np.zeros(max(min(r, c), 1))
+    rc = L.tessera_qa_svd(a.ctypes.data_as(_lib.c_double_p), r, c, s.ctypes.data_as(_lib.c_double_p), None, None)
+    assert rc == _lib.EINVAL
+    assert "shape" in _lib.last_error()
+
+
+@pytest.mark.parametrize("shape", [(0, 4), (257, 4), (4, 257)])
+def test_noalloc_svd_rejects_out_of_range_shapes_without_a_gpu(shape):
+    import ctypes as C
+    L = _lib.load()
+    dummy = C.c_void_p(16)  # never dereferenced: the shape check comes first
+    rc = L.tessera_qa_svd_noalloc(dummy, shape[0], shape[1], dummy, None, None)
+    assert rc == _lib.EINVAL
+    assert "rows and cols" in _lib.last_error()
