@@ -155,3 +155,40 @@ def test_noalloc_svd_rejects_out_of_range_shapes_without_a_gpu(shape):
     rc = L.tessera_qa_svd_noalloc(dummy, shape[0], shape[1], dummy, None, None)
     assert rc == _lib.EINVAL
     assert "rows and cols" in _lib.last_error()
+
+
+def test_null_handles_and_structs_are_rejected_without_a_gpu():
+    """Every handle-taking entry point returns EINVAL (or NULL / 0 / no-op for the void and
+    size-returning ones) on a NULL handle or NULL struct, before any CUDA call."""
+    import ctypes as C
+    L = _lib.load()
+    f0 = C.c_float(0.0)
+    einval = {
+        "session_randomize": lambda: L.tessera_qa_session_randomize(None, 1),
+        "session_run": lambda: L.tessera_qa_session_run(None, 0, 1),
+        "session_run_gates": lambda: L.tessera_qa_session_run_gates(None, 0, 0, 1),
+        "session_run_host": lambda: L.tessera_qa_session_run_host(None, None, 0, 0, 0, 0, None),
+        "session_sync": lambda: L.tessera_qa_session_sync(None, None),
+        "session_observe": lambda: L.tessera_qa_session_observe(None, None),
+        "session_save": lambda: L.tessera_qa_session_save(None, None, 0),
+        "session_load": lambda: L.tessera_qa_session_load(None, None, 0),
+        "session_sample": lambda: L.tessera_qa_session_sample(None, 1, 1, None, None),
+        "session_save_instance": lambda: L.tessera_qa_session_save_instance(None, 0, None, 0),
+        "gnn_get_params": lambda: L.tessera_qa_gnn_get_params(None, None, 0),
+        "gnn_set_params": lambda: L.tessera_qa_gnn_set_params(None, None, 0),
+        "gnn_forward": lambda: L.tessera_qa_gnn_forward(None, None, 0, None, None),
+        "gnn_train_step": lambda: L.tessera_qa_gnn_train_step(None, None, 0, None, None, f0, f0, None, None),
+        "gnn_apply_grads": lambda: L.tessera_qa_gnn_apply_grads(None, None, 0, f0),
+        "schedule_predict": lambda: L.tessera_qa_schedule_predict(None, None, 0, None, None),
+        "anneal_ex": lambda: L.tessera_qa_anneal_ex(None, None, None),
+        "anneal_batch": lambda: L.tessera_qa_anneal_batch(None, None, None, 1),
+        "sv_anneal": lambda: L.tessera_qa_sv_anneal(None, 0.1, 0, None),
+    }
+    for name, call in einval.items():
+        assert call() == _lib.EINVAL, name
+    assert not L.tessera_qa_session_stream(None)
+    assert not L.tessera_qa_session_create(None, None)
+    assert not L.tessera_qa_session_create_batch(None, None, 0)
+    assert L.tessera_qa_gnn_param_count(None) == 0
+    L.tessera_qa_session_destroy(None)
+    L.tessera_qa_gnn_destroy(None)
