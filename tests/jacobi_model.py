@@ -1,0 +1,82 @@
+"""A numpy model of the engine's one-sided Jacobi SVD, for CPU experiments on its rules.
+
+It restates what tessera_b200/csrc/kernels.cu does per column pair: FP64 sums alpha = |x|^2,
+beta = |y|^2, gamma = x^H y; the convergence test |gamma|^2 > tol^2 alpha beta; the noise floor
+tiny = (8 sqrt(R) eps)^2 ||A||_F^2 under which a column is frozen; the complex128 rotation of
+jacobi_rotation (u = (|beta - alpha| + sqrt((beta - alpha)^2 + 4|gamma|^2)) / (2|gamma|),
+c = u w, s = sgn(zeta) w, w = 1/sqrt(u^2 + 1)); and the update x' = c x - s conj(e) y,
+y' = s e x + c y with e = gamma/|gamma|.  Columns are put in descending norm order at every
+sweep and visited in row-cyclic order, as the batched kernel does (it groups them in blocks of
+8, which changes the order of the pairs but not the rules).
+
+freeze rules:
+  "A": skip a pair when either column is under the floor (the kernels);
+  "C": skip only pairs with both columns under the floor;
+  "F": C while a sweep still rotates at least 10% of its pairs, then A.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+EPS64 = 2.220446049250313e-16
+
+
+def rotation(v0, v1, v2, v3):
+    g2 = v2 * v2 + v3 * v3
+    rg = 1.0 / np.sqrt(g2)
+    zeta = 0.5 * (v1 - v0) * rg
+    d = v1 - v0
+    u = 0.5 * rg * (abs(d) + np.sqrt(d * d + 4.0 * g2))
+    w = 1.0 / np.sqrt(u * u + 1.0)
+    return u * w, (w if zeta >= 0 else -w), complex(v2 * rg, v3 * rg)
+
+
+def one_sided_jacobi(A: np.ndarray, rule: str = "A", tol: float = 1e-13, max_sweeps: int = 60):
+    """Returns (sigma descending, W with columns in the same order, sweeps, floor)."""
+    W = np.array(A, dtype=np.complex128, copy=True)
+    R, N = W.shape
+    fro2 = float(np.sum(np.abs(W) ** 2))
+    tiny = max(1e-200, (8.0 * np.sqrt(R) * EPS64) ** 2 * fro2)
+    late = rule == "A"
+    sweeps = max_sweeps
+    for sweep in range(max_sweeps):
+        W = W[:, np.argsort(-np.sum(np.abs(W) ** 2, axis=0), kind="stable")]
+        rot = 0
+        for i in range(N - 1):
+            for j in range(i + 1, N):
+                x, y = W[:, i], W[:, j]
+                v0 = float(np.vdot(x, x).real)
+                v1 = float(np.vdot(y, y).real)
+                g = np.vdot(x, y)
+                v2, v3 = float(g.real), float(g.imag)
+                if late or rule == "A":
+                    if not (v0 > tiny and v1 > tiny):
+                        continue
+                elif not (v0 > tiny or v1 > tiny):
+                    continue
+                if not (v2 * v2 + v3 * v3 > tol * tol * v0 * v1):
+                    continue
+                c, s, e = rotation(v0, v1, v2, v3)
+                xn = c * x - s * np.conj(e) * y  # both from the old columns (x, y are views)
+                yn = s * e * x + c * y
+                W[:, i] = xn
+                W[:, j] = yn
+                rot += 1
+        if rule == "F" and not late and rot < 0.1 * N * (N - 1) / 2:
+            late = True
+            continue
+        if rot == 0:
+            sweeps = sweep + 1
+            break
+    sig = np.sqrt(np.sum(np.abs(W) ** 2, axis=0))
+    order = np.argsort(-sig, kind="stable")
+    return sig[order], W[:, order], sweeps, float(np.sqrt(tiny))
+
+
+def graded(n: int, decay: float, seed: int) -> tuple[np.ndarray, np.ndarray]:
+    """n x n matrix U diag(exp(-k/decay)) V^H with Haar-like random unitary U, V."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    X = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+    U, _, Vh = np.linalg.svd(X)
+    s = np.exp(-np.arange(n) / decay)
+    return (U * s) @ Vh, s

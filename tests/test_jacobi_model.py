@@ -1,0 +1,54 @@
+"""The freeze rules of the one-sided Jacobi, on the numpy model of the kernels (tests/jacobi_model.py).
+
+Rule A (the kernels: a column under the noise floor is never rotated again) lets a column
+whose norm dips under the floor mid-sweep stay frozen, so singular values a few times the
+floor come back wrong.  Rule F (rotate every pair with one column above the floor while a
+sweep still rotates >= 10% of its pairs, then rule A) resolves them at the same sweep count.
+"""
+import numpy as np
+import pytest
+
+from jacobi_model import graded, one_sided_jacobi
+
+
+@pytest.fixture(scope="module")
+def runs():
+    A, s = graded(96, 2.5, 7)
+    return s, {rule: one_sided_jacobi(A, rule) for rule in ("A", "F")}
+
+
+def _rel_err_above(s, sig, floor, k=4.0):
+    keep = s > k * floor
+    return float(np.max(np.abs(sig[keep] - s[keep]) / s[keep]))
+
+
+def test_rule_a_loses_values_above_the_floor(runs):
+    s, r = runs
+    sig, _, _, floor = r["A"]
+    assert _rel_err_above(s, sig, floor) > 1e-3
+
+
+def test_rule_f_resolves_them_at_the_same_cost(runs):
+    s, r = runs
+    sig_f, W, sweeps_f, floor = r["F"]
+    _, _, sweeps_a, _ = r["A"]
+    assert _rel_err_above(s, sig_f, floor) < 1e-4
+    assert np.max(np.abs(sig_f - s)) < floor  # everything else within the floor
+    assert sweeps_f <= sweeps_a + 2
+    kept = sig_f > floor
+    U = W[:, kept] / sig_f[kept]
+    assert np.linalg.norm(U.conj().T @ U - np.eye(U.shape[1])) < 1e-10
+
+
+def test_model_rotation_matches_the_textbook_form():
+    rng = np.random.default_rng(3)
+    from jacobi_model import rotation
+    for _ in range(200):
+        v0, v1 = 10 ** rng.uniform(-3, 3, 2)
+        g = np.sqrt(v0 * v1) * 10 ** rng.uniform(-6, 0)
+        ph = rng.uniform(0, 2 * np.pi)
+        c, s, e = rotation(v0, v1, g * np.cos(ph), g * np.sin(ph))
+        zeta = 0.5 * (v1 - v0) / g
+        t = np.sign(zeta if zeta != 0 else 1.0) / (abs(zeta) + np.sqrt(1 + zeta * zeta))
+        assert c == pytest.approx(1 / np.sqrt(1 + t * t), rel=1e-14)
+        assert s == pytest.approx(t / np.sqrt(1 + t * t), rel=1e-13, abs=1e-300)
