@@ -617,6 +617,74 @@ int orc_mps_anneal(const double* h, int n, const int* ei, const int* ej, const d
     return 0;
 }
 
+// Gate slots [q0, q1) of one step's ZZ block applied to a given MPS.  The slots are the
+// two-site updates of the block in the reference's order: edges in list order (reverse order
+// on odd substeps, cuda/src/mps.cpp:330-341), each through the swap network of
+// cuda/src/mps.cpp:126-145 (swaps on bonds k-1 for k = j..i+2, the ZZ gate on bond i, swaps back
+// on bonds k for k = i+1..j-1), the ZZ angle -B w dt/ns.  Every slot is apply_adjacent
+// (cuda/src/mps.cpp:41-100): keep rule, discarded weight and gauge A <- U, C <- S Vh.
+// dims: n+1 bond dimensions; sites: the n site tensors (Dl, 2, Dr) back to back, interleaved
+// complex, element (a, s, b) at (a*2 + s)*Dr + b -- the payload of the engine's checkpoint.
+// Writes the updated dims and sites (out_cap doubles available; returns -1 when too small,
+// else the number of doubles written).  stats = {max_trunc, updates, min relative cut gap,
+// max SVD reconstruction error}.
+long long orc_mps_apply_slots(int n, const int* dims, const double* sites, const int* ei, const int* ej,
+                              const double* ew, int m, double B, double dt, int zz_substeps, int chi,
+                              int q0, int q1, int svd_mode, int* out_dims, double* out_sites,
+                              long long out_cap, double* stats) {
+    Chain psi(n);
+    psi.svd_mode = svd_mode;
+    size_t off = 0;
+    for (int i = 0; i < n; ++i) {
+        Tensor3 t(dims[i], dims[i + 1]);
+        for (size_t e = 0; e < t.t.size(); ++e, ++off) t.t[e] = cplx(sites[2 * off], sites[2 * off + 1]);
+        psi.site[i] = std::move(t);
+    }
+    struct Slot { int bond; bool zz; double theta; };
+    std::vector<Slot> slots;
+    const int ns = zz_substeps < 1 ? 1 : zz_substeps;
+    const double sub = dt / ns;
+    for (int sstep = 0; sstep < ns; ++sstep)
+        for (int q = 0; q < m; ++q) {
+            const int e = (sstep % 2 == 0) ? q : m - 1 - q;
+            int i = ei[e], j = ej[e];
+            if (i > j) std::swap(i, j);
+            if (i == j) continue;
+            const double th = -B * ew[e] * sub;
+            for (int k = j; k > i + 1; --k) slots.push_back({k - 1, false, 0.0});
+            slots.push_back({i, true, th});
+            for (int k = i + 1; k < j; ++k) slots.push_back({k, false, 0.0});
+        }
+    if (q0 < 0 || q1 > (int)slots.size() || q0 > q1) return -2;
+    cplx W[4][4] = {};
+    W[0][0] = 1; W[1][2] = 1; W[2][1] = 1; W[3][3] = 1;
+    for (int q = q0; q < q1; ++q) {
+        const Slot& sl = slots[q];
+        if (sl.zz) {
+            cplx Z[4][4] = {};
+            const cplx ph = std::exp(cplx(0, -sl.theta)), phc = std::exp(cplx(0, sl.theta));
+            Z[0][0] = ph; Z[1][1] = phc; Z[2][2] = phc; Z[3][3] = ph;
+            psi.two_site(sl.bond, Z, chi);
+        } else {
+            psi.two_site(sl.bond, W, chi);
+        }
+    }
+    long long need = 0;
+    for (int i = 0; i < n; ++i) need += 2LL * (long long)psi.site[i].t.size();
+    if (need > out_cap) return -1;
+    out_dims[0] = 1;
+    size_t o = 0;
+    for (int i = 0; i < n; ++i) {
+        out_dims[i + 1] = psi.site[i].dr;
+        for (const cplx& z : psi.site[i].t) { out_sites[o++] = z.real(); out_sites[o++] = z.imag(); }
+    }
+    stats[0] = psi.max_trunc;
+    stats[1] = (double)psi.updates;
+    stats[2] = psi.min_gap;
+    stats[3] = psi.max_recon;
+    return need;
+}
+
 // Gram-matrix thin SVD restatement (cuda/src/linalg.cpp:107-172); row-major interleaved.
 int orc_svd(int rows, int cols, const double* a, double* s, double* u, double* vh) {
     Dense A(rows, cols);

@@ -190,3 +190,35 @@ def test_reference_live_matches_oracle_when_built(oracle):
     r2 = oracle.mps_anneal(inst, p.sa, p.sb, p.dt, 4)
     assert r1.energy == r2.energy and r1.max_trunc == pytest.approx(r2.max_trunc, rel=1e-9)
     assert np.max(np.abs(r1.entropy - r2.entropy)) < 1e-10
+
+
+def test_apply_slots_equals_zz_phases_on_the_dense_state(oracle):
+    """orc_mps_apply_slots (gate slots of one step's ZZ block on a given MPS) at exact bond
+    dimension: the swap network moves sites and moves them back, so after all slots of the block
+    the state is the input times exp(-i theta_e Z_i Z_j) for every edge, theta_e = -B w_e dt
+    (cuda/src/mps.cpp:116-145, 330-341).  A random MPS of 7 sites, couplings to distance 3."""
+    from tessera_b200 import ffi
+    rng = np.random.default_rng(5)
+    n = 7
+    dims = [1] + [2 ** min(i, n - i) for i in range(1, n)] + [1]
+    sites = [rng.normal(size=(dims[i], 2, dims[i + 1])) + 1j * rng.normal(size=(dims[i], 2, dims[i + 1]))
+             for i in range(n)]
+    p = instances.chain_range(n=n, dmax=3, seed=4, T=1.0, dt=0.1, chi=8, dist="normal")
+    inst = Instance(p.h, p.ei.astype(np.int32), p.ej.astype(np.int32), p.ew)
+    nslots = sum(2 * abs(int(j) - int(i)) - 1 for i, j in zip(p.ei, p.ej))
+    B, dt = 0.7, 0.1
+    out, st = oracle.apply_slots(inst, sites, B, dt, 8, 0, nslots)
+    assert st["updates"] == nslots and st["max_trunc"] < 1e-28
+    psi = ffi.sites_to_dense(sites)
+    x = np.arange(1 << n)
+    z = 1 - 2 * ((x[:, None] >> np.arange(n)) & 1)  # physical index 0 <-> spin +1
+    phase = np.zeros(1 << n)
+    for i, j, w in zip(p.ei, p.ej, p.ew):
+        phase += -B * w * dt * z[:, i] * z[:, j]
+    want = psi * np.exp(-1j * phase)
+    got = ffi.sites_to_dense(out)
+    assert np.linalg.norm(got - want) < 1e-12 * np.linalg.norm(want)
+    # slots 2..4 are updates on bonds 0, 1, 2 (edges (0,2) and (0,3)): sites 4.. are untouched
+    part, st2 = oracle.apply_slots(inst, sites, B, dt, 8, 2, 5)
+    assert st2["updates"] == 3
+    assert all(np.array_equal(part[i], sites[i]) for i in range(4, n))
