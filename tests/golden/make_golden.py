@@ -3,7 +3,7 @@
 Run where the reference sources are mounted (they are compiled by oracle/Makefile into
 oracle/_ref/libtessera_ref.so):
 
-    make -C oracle && python tests/golden/make_golden.py
+    TESSERA_REF_ROOT=<reference checkout> make -C oracle && python tests/golden/make_golden.py
 
 Writes reference_cases.json: every case holds its inputs (instance, schedule, dt, chi,
 zz_substeps) and the reference's outputs (spins, energy, expected_energy, prob,
