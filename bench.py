@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--batch", type=int, default=148, help="instances per GPU (1 = plain single-instance engine)")
     ap.add_argument("--gates", type=int, default=8, help="gate slots per bench step")
     ap.add_argument("--impl", choices=["tessera", "reference"], default="tessera")
+    ap.add_argument("--ref-chi", type=int, default=128,
+                    help="bond dimension the reference arm times (extrapolated to --chi when smaller)")
     ap.add_argument("--precision", choices=["c128", "c64"], default="c128")
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--dmax", type=int, default=4)
@@ -179,50 +181,68 @@ class Clocks:
 # ------------------------------------------------------------------------------------
 # reference CPU engine (oracle/_ref: the reference's own sources compiled here)
 # ------------------------------------------------------------------------------------
-def ref_svd_sample(m: int, threads: int, seed: int = 0):
-    """Wall time of `threads` concurrent reference tessera::svd calls on m x m complex matrices
-    with a TEBD-like decaying spectrum (one per thread; ctypes releases the GIL)."""
-    import numpy as np
-
+def ref_update_sample(chi: int, threads: int, seed: int = 0):
+    """Wall time of `threads` concurrent saturated-bond updates through the reference's own
+    MPS::apply_adjacent (cuda/src/mps.cpp:41-100), one per thread on a (2 chi) x (2 chi) theta
+    (ctypes releases the GIL); returns (wall seconds, per-update seconds)."""
     from oracle.oracle import Reference
     R = Reference()
-    rng = np.random.Generator(np.random.PCG64(seed))
-    mats = []
-    for _ in range(threads):
-        A = rng.normal(size=(m, m)) + 1j * rng.normal(size=(m, m))
-        U, _, Vh = np.linalg.svd(A)
-        mats.append((U * np.exp(-np.arange(m) / (m / 8))) @ Vh)
-    ths = [threading.Thread(target=R.svd, args=(a,)) for a in mats]
+    per = [0.0] * threads
+
+    def one(k):
+        sec, _ = R.saturated_update(chi, 1, seed + k)
+        per[k] = float(sec[0])
+
+    ths = [threading.Thread(target=one, args=(k,)) for k in range(threads)]
     t0 = time.perf_counter()
     for t in ths:
         t.start()
     for t in ths:
         t.join()
-    return time.perf_counter() - t0
+    return time.perf_counter() - t0, per
+
+
+REF_DIRECT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "reference_update_chi256.json")
 
 
 class RefModel:
-    """Reference cost of one saturated chi=256 update: tessera::svd of a 512 x 512 theta is
-    >99% of MPS::apply_adjacent at that size (cuda/src/mps.cpp:41-100).  A step times m=256
-    (chi=128) SVDs on every host thread at once and extrapolates to m=512 with the cost
-    exponent between one m=128 SVD (timed once) and the m=256 batch."""
+    """Reference cost of saturated chi=256 updates on the host cores.  A direct chi=256 update
+    (512 x 512 theta, MPS::apply_adjacent) takes minutes on one core, so by default a step times
+    one chi=128 update (256 x 256 theta) on every host thread at once and extrapolates to
+    chi=256 with the cost exponent between chi=64 and chi=128, both measured at the same
+    concurrency.  --ref-chi 256 times chi=256 updates directly (no extrapolation); the record of
+    such a run (profiles/reference_update_chi256.json) is quoted beside the extrapolated value."""
 
-    def __init__(self):
+    def __init__(self, chi: int = 128, target: int = 256):
         self.threads = max(1, min(len(os.sched_getaffinity(0)), 64))
-        self.t128 = ref_svd_sample(128, 1, seed=1)
-        self.p = 4.0
+        self.chi, self.target = chi, target
+        self.p = 3.0
+        self.t_lo = None
+        if chi < target:
+            self.t_lo, _ = ref_update_sample(chi // 2, self.threads, seed=1)
 
     def step(self, seed=3):
         import math
-        t = ref_svd_sample(256, self.threads, seed=seed)
-        self.p = math.log2(t / self.t128)
-        per_update_512 = t * 2.0 ** self.p
-        return t, self.threads / per_update_512
+        t, per = ref_update_sample(self.chi, self.threads, seed=seed)
+        if self.chi >= self.target:
+            return t, self.threads / t
+        self.p = math.log2(t / self.t_lo)
+        return t, self.threads / (t * (self.target / self.chi) ** self.p)
 
     def describe(self, t):
-        return (f"{self.threads} concurrent reference tessera::svd calls on 256x256 complex128 theta "
-                f"(chi=128) took {t:.1f} s; extrapolated to the 512x512 theta of chi=256 with the "
-                f"measured cost exponent {self.p:.2f} (one 128x128 SVD -> the 256x256 batch)")
+        if self.chi >= self.target:
+            return (f"{self.threads} concurrent reference MPS::apply_adjacent updates of a saturated chi={self.chi} "
+                    f"bond ({2 * self.chi}x{2 * self.chi} complex128 theta), measured directly: {t:.1f} s")
+        d = (f"{self.threads} concurrent reference MPS::apply_adjacent updates of a saturated chi={self.chi} bond "
+             f"({2 * self.chi}x{2 * self.chi} complex128 theta) took {t:.1f} s; extrapolated to chi={self.target} "
+             f"with the cost exponent {self.p:.2f} measured between chi={self.chi // 2} ({self.t_lo:.2f} s) and "
+             f"chi={self.chi} at the same concurrency")
+        if os.path.exists(REF_DIRECT):
+            with open(REF_DIRECT) as f:
+                rd = json.load(f)
+            d += (f"; a direct chi={rd['chi']} measurement on this pool ({rd['threads']} threads, "
+                  f"{rd['seconds']:.0f} s wall) gave {rd['value']:.4g} updates/s")
+        return d
 
 
 def run_reference(args):
@@ -233,7 +253,7 @@ def run_reference(args):
     if not Reference.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libtessera_ref.so was not built"}))
         return
-    model = RefModel()
+    model = RefModel(chi=min(args.ref_chi, args.chi), target=args.chi)
     for w in range(args.warmup):
         model.step(seed=10 + w)
     vals, walls = [], []
@@ -522,7 +542,7 @@ def main():
         try:
             from oracle.oracle import Reference
             if Reference.available():
-                model = RefModel()
+                model = RefModel(chi=min(args.ref_chi, args.chi), target=args.chi)
                 tw, v = model.step()
                 cpu = {"value": v, "unit": UNIT, "cores": model.threads, "kind": "reference",
                        "sample": model.describe(tw)}

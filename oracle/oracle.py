@@ -102,6 +102,10 @@ class Oracle:
         L.orc_exact_ground.argtypes = [_dp, C.c_int, _ip, _ip, _dp, C.c_int, _i8p]
         L.orc_exact_ground.restype = C.c_double
         L.orc_svd.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp]
+        L.orc_mps_apply_slots.argtypes = [C.c_int, _ip, _dp, _ip, _ip, _dp, C.c_int, C.c_double, C.c_double,
+                                          C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _ip, _dp,
+                                          C.c_longlong, _dp]
+        L.orc_mps_apply_slots.restype = C.c_longlong
         L.orc_hermitian_eig.argtypes = [C.c_int, _dp, _dp, _dp]
         L.orc_hermitian_expm.argtypes = [C.c_int, _dp, C.c_double, C.c_double, _dp]
         L.orc_mt_dense_instance.argtypes = [C.c_ulonglong, C.c_int, C.c_int, C.c_int, _dp, _ip,
@@ -126,6 +130,34 @@ class Oracle:
                          state.view(np.complex128) if state is not None else None,
                          extra={"max_recon": st[6], "bad_updates": int(st[7]), "norm2": st[8],
                                 "min_cut_gap": st[9]})
+
+    def apply_slots(self, inst: Instance, sites, B: float, dt: float, chi: int, q0: int, q1: int,
+                    zz_substeps: int = 1, accurate_svd: bool = True):
+        """Gate slots [q0, q1) of one step's ZZ block (ZZ weight B) applied to the MPS given as a
+        list of site tensors (Dl, 2, Dr); returns (sites, stats) with stats = {max_trunc,
+        updates, min_cut_gap, max_recon}.  The slot order is the reference's gate order through
+        the swap network, the update its apply_adjacent (cuda/src/mps.cpp:41-145, 330-341)."""
+        ei, ej, ew = _i(inst.ei), _i(inst.ej), _d(inst.ew)
+        n = len(sites)
+        dims = np.array([1] + [int(t.shape[2]) for t in sites], np.int32)
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(t, np.complex128).reshape(-1) for t in sites]))
+        cap = 2 * sum(int(dims[i]) * 2 * max(int(dims[i + 1]), chi) * 2 for i in range(n)) + 64
+        out = np.zeros(cap)
+        odims = np.zeros(n + 1, np.int32)
+        st = np.zeros(4)
+        rc = self.lib.orc_mps_apply_slots(n, _ptr(dims, _ip), _ptr(flat.view(np.float64), _dp), _ptr(ei, _ip),
+                                          _ptr(ej, _ip), _ptr(ew, _dp), len(ew), B, dt, zz_substeps, chi, q0, q1,
+                                          1 if accurate_svd else 0, _ptr(odims, _ip), _ptr(out, _dp), cap,
+                                          _ptr(st, _dp))
+        if rc < 0:
+            raise ValueError(f"orc_mps_apply_slots failed ({rc})")
+        z = out[:rc].view(np.complex128)
+        res, off = [], 0
+        for i in range(n):
+            cnt = int(odims[i]) * 2 * int(odims[i + 1])
+            res.append(z[off:off + cnt].reshape(odims[i], 2, odims[i + 1]).copy())
+            off += cnt
+        return res, {"max_trunc": st[0], "updates": int(st[1]), "min_cut_gap": st[2], "max_recon": st[3]}
 
     def sv_anneal(self, inst: Instance, sa, sb, dt: float, mode: int = 0,
                   want_state: bool = False, bias=None, sc=None) -> AnnealOut:
@@ -212,6 +244,9 @@ class Reference:
         L.ref_grow_and_apply.argtypes = [C.c_int, C.c_int, C.c_int, _dp, C.c_int, C.c_int, C.c_int,
                                          C.c_double, C.c_int, _dp]
         L.ref_grow_and_apply.restype = C.c_int
+        if hasattr(L, "ref_saturated_update"):
+            L.ref_saturated_update.argtypes = [C.c_int, C.c_int, C.c_ulonglong, _dp, _dp]
+            L.ref_saturated_update.restype = C.c_int
         L.tessera_qa_anneal.argtypes = [_dp, C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
                                         _dp, C.c_size_t, _dp, _dp, C.c_size_t, C.c_size_t, _i8p, _dp]
         L.tessera_qa_anneal.restype = C.c_double
@@ -272,6 +307,14 @@ class Reference:
         self.lib.ref_hermitian_expm(n, _ptr(a.view(np.float64), _dp), coeff.real, coeff.imag,
                                     _ptr(out.view(np.float64), _dp))
         return out
+
+    def saturated_update(self, chi: int, reps: int = 1, seed: int = 0):
+        """Wall times of `reps` updates of a saturated bond (theta (2 chi) x (2 chi)) through the
+        reference's own MPS::apply_adjacent (cuda/src/mps.cpp:41-100); returns (seconds, bond)."""
+        sec = np.zeros(reps)
+        tr = np.zeros(1)
+        bond = self.lib.ref_saturated_update(chi, reps, seed, _ptr(sec, _dp), _ptr(tr, _dp))
+        return sec, int(bond)
 
     def grow_and_apply(self, n, chi, layers, gates: np.ndarray, zz_i, zz_j, theta, reps):
         g = np.ascontiguousarray(gates, dtype=np.complex128)

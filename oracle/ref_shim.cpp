@@ -7,11 +7,20 @@
 // returns only the readout energy; the parity tests need the other AnnealResult fields
 // (cuda/include/mps.hpp:37-44) and a caller-chosen dt / zz_substeps
 // (cuda/include/mps.hpp:76-82).
-#include "mps.hpp"
-#include "linalg.hpp"
+#include <chrono>
+#include <complex>
 #include <cstdint>
 #include <cstring>
+#include <random>
 #include <vector>
+// The reference's MPS keeps its site tensors private and offers no way to load a state; the
+// saturated-bond timing below (ref_saturated_update) places random site tensors into it, so
+// this one translation unit sees the class's members as public.  The class layout, the member
+// functions compiled from the reference's mps.cpp and their behaviour are unchanged.
+#define private public
+#include "mps.hpp"
+#undef private
+#include "linalg.hpp"
 
 using namespace tessera;
 
@@ -94,6 +103,37 @@ int ref_grow_and_apply(int n, int chi, int layers, const double* gates, int ngat
     for (int r = 0; r < zz_reps; ++r) psi.apply_zz(zz_i, zz_j, zz_theta, chi, trunc);
     if (trunc_out) *trunc_out = trunc;
     return psi.max_bond();
+}
+
+// One saturated-bond update through the reference's own MPS::apply_adjacent
+// (cuda/src/mps.cpp:41-100): a 4-site MPS with bond dimensions (1, chi, chi, chi, 1) filled
+// with seeded Gaussian complex entries, then `reps` updates of the interior bond (1, 2) --
+// theta is (2 chi) x (2 chi) -- with the ZZ gate exp(-i 0.3 Z Z) and cap chi, alternating
+// with a SWAP so that the bond stays saturated.  Writes the wall time of each update to
+// seconds[reps] and returns the bond dimension after the last one.
+int ref_saturated_update(int chi, int reps, unsigned long long seed, double* seconds, double* trunc_out) {
+    MPS psi(4);
+    std::mt19937_64 g(seed);
+    std::normal_distribution<double> nd(0.0, 1.0);
+    const int dims[5] = {1, chi, chi, chi, 1};
+    for (int i = 0; i < 4; ++i) {
+        Site st(dims[i], dims[i + 1]);
+        const double sc = 1.0 / std::sqrt(2.0 * dims[i]);
+        for (auto& z : st.t) z = cd(nd(g) * sc, nd(g) * sc);
+        psi.s_[i] = st;
+    }
+    cd Z[4][4] = {}, W[4][4] = {};
+    const cd ph = std::exp(cd(0, -0.3)), phc = std::exp(cd(0, 0.3));
+    Z[0][0] = ph; Z[1][1] = phc; Z[2][2] = phc; Z[3][3] = ph;
+    W[0][0] = 1; W[1][2] = 1; W[2][1] = 1; W[3][3] = 1;
+    double trunc = 0.0;
+    for (int r = 0; r < reps; ++r) {
+        const auto t0 = std::chrono::steady_clock::now();
+        psi.apply_adjacent(1, (r % 2) ? W : Z, chi, trunc);
+        seconds[r] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    if (trunc_out) *trunc_out = trunc;
+    return psi.s_[1].Dr;
 }
 
 }  // extern "C"

@@ -1,8 +1,10 @@
 """The JSON line of `bench.py --impl reference` on CPU: its keys, units and the extrapolation.
 
-The reference's own SVD sample (about 20 s per step on 16 threads) is replaced by a stub that
-returns fixed wall times, so only the line's assembly is under test: rank 0 alone prints one
-line; other ranks print nothing; value = threads / (t256 * 2^p) with p = log2(t256 / t128).
+The reference's own update sample (concurrent MPS::apply_adjacent calls on saturated bonds,
+about 20 s per step at chi=128) is replaced by a stub that returns fixed wall times, so only
+the line's assembly is under test: rank 0 alone prints one line; other ranks print nothing;
+value = threads / (t128 * 2^p) with p = log2(t128 / t64), both at the same concurrency; with
+--ref-chi 256 the chi=256 time is used directly.
 """
 import io
 import json
@@ -20,8 +22,8 @@ def _run(monkeypatch, argv, rank="0"):
     monkeypatch.setattr(sys, "argv", ["bench.py"] + argv)
     monkeypatch.setenv("RANK", rank)
     monkeypatch.setattr(orc.Reference, "available", staticmethod(lambda: True))
-    times = {128: 0.05, 256: 0.8}
-    monkeypatch.setattr(bench, "ref_svd_sample", lambda m, threads, seed=0: times[m])
+    times = {64: 0.05, 128: 0.8, 256: 9.0}
+    monkeypatch.setattr(bench, "ref_update_sample", lambda chi, threads, seed=0: (times[chi], [times[chi]] * threads))
     out = io.StringIO()
     with redirect_stdout(out):
         bench.run_reference(bench.parse())
@@ -44,7 +46,7 @@ def test_reference_line_keys_and_value(monkeypatch):
     assert d["ms_per_step"] == pytest.approx(800.0)
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["value"] == d["value"] and cb["unit"] == bench.UNIT
-    assert "extrapolated" in cb["sample"]
+    assert "extrapolated" in cb["sample"] and "same concurrency" in cb["sample"]
     e = d["e2e"]
     assert e["value"] == d["value"] and e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
     assert d["config"]["chi"] == 256 and d["config"]["updates_per_trotter_step"] == 1998
@@ -52,3 +54,10 @@ def test_reference_line_keys_and_value(monkeypatch):
 
 def test_reference_line_only_on_rank_zero(monkeypatch):
     assert _run(monkeypatch, ["--impl", "reference", "--steps", "1", "--warmup", "0"], rank="1") == ""
+
+
+def test_reference_line_direct_chi256(monkeypatch):
+    text = _run(monkeypatch, ["--impl", "reference", "--steps", "1", "--warmup", "0", "--ref-chi", "256"])
+    d = json.loads(text.strip())
+    assert d["value"] == pytest.approx(d["cpu_baseline"]["cores"] / 9.0)
+    assert "measured directly" in d["cpu_baseline"]["sample"]
