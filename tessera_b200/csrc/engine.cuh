@@ -82,7 +82,7 @@ struct SvdParams {
     int no_trunc;      // 1: keep all min(R, N) values, leave dims and run statistics alone
     int chi;
     double tol;
-    double tiny;       // columns with |w|^2 below this are never rotated
+    double tiny;       // absolute lower bound of the noise floor on |w|^2 (pair_live)
     int max_sweeps;
     int rows_cap;      // shared-memory column length
     int cols_cap;      // shared-memory column count of the resident Jacobi (>= N, even)

@@ -284,10 +284,28 @@ __device__ __forceinline__ void group_reduce4(double v[4], double* red, int tid)
     }
 }
 
+// Freeze rule for columns under the noise floor `tiny` (on |w|^2).  In the early phase of an
+// SVD ("mixed": the previous sweep still rotated at least 10% of the N(N-1)/2 pairs) a pair is
+// live when one column is above the floor and the other holds more than 1e-6 of it; after
+// that, only when both columns are above the floor.  A column whose norm dips under the floor
+// mid-sweep is thereby still orthogonalised against the resolved columns, so values a few
+// times the floor come back right, while noise columns (rank-deficient or wide theta) are
+// dropped as soon as the sweeps settle.  The 1e-6 margin also bounds the ratio of the two
+// norms, so the rotation below cannot overflow.
+__device__ __forceinline__ bool pair_live(const double v0, const double v1, const double tiny, const bool mixed) {
+    const double lo = fmin(v0, v1);
+    return mixed ? (fmax(v0, v1) > tiny && lo > 1e-6 * tiny) : lo > tiny;
+}
+
+// Whether the next sweep stays in the mixed phase, from this sweep's rotation count.
+__device__ __forceinline__ bool still_mixed(const bool mixed, const double rotated, const int N) {
+    return mixed && rotated >= 0.05 * (double)N * (double)(N - 1);
+}
+
 // Rotation of a column pair from alpha = |w_p|^2 (v0), beta = |w_q|^2 (v1) and
 // gamma = w_p^H w_q (v2 + i v3), all accumulated in FP64.  Returns false for a converged
-// pair (|gamma|^2 <= tol^2 alpha beta, the FP64 convergence test) or a column below the
-// noise floor; else c, s and the phase e = gamma/|gamma| of
+// pair (|gamma|^2 <= tol^2 alpha beta, the FP64 convergence test) or a pair that the freeze
+// rule (pair_live) leaves alone; else c, s and the phase e = gamma/|gamma| of
 //   w_p <- c w_p - s conj(e) w_q,   w_q <- s e w_p + c w_q,
 //   zeta = (beta - alpha) / (2|gamma|), t = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)),
 //   c = 1/sqrt(1 + t^2), s = c t.
@@ -295,9 +313,10 @@ __device__ __forceinline__ void group_reduce4(double v[4], double* red, int tid)
 // (the precision they are applied in).
 template <typename T>
 __device__ __forceinline__ bool jacobi_rotation(const double v0, const double v1, const double v2, const double v3,
-                                                const double tol, const double tiny, T& c, T& s, T& er, T& ei) {
+                                                const double tol, const double tiny, const bool mixed, T& c, T& s,
+                                                T& er, T& ei) {
     const double g2 = v2 * v2 + v3 * v3;
-    if (!(v0 > tiny && v1 > tiny && g2 > tol * tol * (v0 * v1))) return false;
+    if (!(pair_live(v0, v1, tiny, mixed) && g2 > tol * tol * (v0 * v1))) return false;
     const double rg = rsqrt(g2);
     const double zeta = 0.5 * (v1 - v0) * rg;
     er = (T)(v2 * rg);
@@ -326,7 +345,7 @@ __device__ __forceinline__ bool jacobi_rotation(const double v0, const double v1
 // Rotate local columns p, q (shared memory) of a group; returns 1 if rotated.
 template <typename T, int G>
 __device__ __forceinline__ int rotate_pair(cplx_t<T>* cp, cplx_t<T>* cq, bool valid, int R, double tol,
-                                           double tiny, double* red, int tid) {
+                                           double tiny, bool mixed, double* red, int tid) {
     using V = cplx_t<T>;
     const int lg = tid % G;
     double v[4] = {0.0, 0.0, 0.0, 0.0};
@@ -342,7 +361,7 @@ __device__ __forceinline__ int rotate_pair(cplx_t<T>* cp, cplx_t<T>* cq, bool va
     group_reduce4<G>(v, red, tid);
     if (!valid) return 0;
     T cc, ss, er, ei;
-    if (!jacobi_rotation<T>(v[0], v[1], v[2], v[3], tol, tiny, cc, ss, er, ei)) return 0;
+    if (!jacobi_rotation<T>(v[0], v[1], v[2], v[3], tol, tiny, mixed, cc, ss, er, ei)) return 0;
     for (int r = lg; r < R; r += G) {
         const V x = cp[r], y = cq[r];
         // s conj(e) y and s e x
@@ -518,7 +537,7 @@ __device__ __forceinline__ void svd_body(const MpsView<T>& mps, const SvdWork<T>
         __syncthreads();
     }
     // ||W||_F^2 first: columns whose squared norm is below the noise floor of the matrix
-    // (tiny) are never rotated, and the keep rule drops them.
+    // (tiny) are left alone once the sweeps settle (pair_live), and the keep rule drops them.
     {
         const int warp = tid >> 5, lane = tid & 31;
         double part = 0.0;
@@ -539,14 +558,16 @@ __device__ __forceinline__ void svd_body(const MpsView<T>& mps, const SvdWork<T>
     if (!cta_sync(wk.bar, status, nblk)) return;
     const double fro2 = *(volatile double*)&wk.scal[0];
     // Noise floor: a column whose norm is below 8 sqrt(R) ulps of ||W||_F carries only rounding
-    // noise; it is frozen (never rotated) and dropped by the keep rule.  Rotating such columns
-    // against each other never converges and costs many sweeps on rank-deficient theta.
+    // noise and is dropped by the keep rule; pairs of such columns are never rotated (that never
+    // converges and costs many sweeps on rank-deficient theta), and pairs with one of them only
+    // in the early sweeps (pair_live).
     const double ulp = sizeof(T) == 8 ? 2.220446049250313e-16 : 1.1920928955078125e-07;
     const double floor_rel = 8.0 * sqrt((double)R) * ulp;
     const double tiny = fmax(pp.tiny, floor_rel * floor_rel * fro2);
     const double keep_floor = fmax(1e-28, tiny);  // on sigma^2: the reference's 1e-14, or the noise floor
     int sweep = 0;
     bool converged = false;
+    bool mixed = true;
     for (; sweep < pp.max_sweeps; ++sweep) {
         for (int r = 0; r < P - 1; ++r) {
             for (int pr = cta; pr < P / 2; pr += ncta) {
@@ -589,7 +610,7 @@ __device__ __forceinline__ void svd_body(const MpsView<T>& mps, const SvdWork<T>
                         const int base = blk ? J * BW : I * BW;
                         const bool ok = (base + x < N) && (base + y < N);
                         rot += rotate_pair<T, G>(col + (blk * BW + x) * pp.rows_cap, col + (blk * BW + y) * pp.rows_cap,
-                                                 ok, R, pp.tol, tiny, red, tid);
+                                                 ok, R, pp.tol, tiny, mixed, red, tid);
                         __syncthreads();
                     }
                 }
@@ -598,7 +619,7 @@ __device__ __forceinline__ void svd_body(const MpsView<T>& mps, const SvdWork<T>
                         const int p = grp, q = (grp + t) % BW;
                         const bool ok = (I * BW + p < N) && (J * BW + q < N);
                         rot += rotate_pair<T, G>(col + p * pp.rows_cap, col + (BW + q) * pp.rows_cap, ok, R, pp.tol,
-                                                 tiny, red, tid);
+                                                 tiny, mixed, red, tid);
                         __syncthreads();
                     }
                 } else {
@@ -639,7 +660,7 @@ __device__ __forceinline__ void svd_body(const MpsView<T>& mps, const SvdWork<T>
                             v3 += __shfl_xor_sync(0xffffffffu, v3, o);
                         }
                         T c, sn, er, ei;
-                        if (ok && jacobi_rotation<T>(v0, v1, v2, v3, pp.tol, tiny, c, sn, er, ei)) {
+                        if (ok && jacobi_rotation<T>(v0, v1, v2, v3, pp.tol, tiny, mixed, c, sn, er, ei)) {
 #pragma unroll
                             for (int k = 0; k < RPL; ++k) {
                                 const V x = xi[k], y = yj[k];
@@ -684,6 +705,7 @@ __device__ __forceinline__ void svd_body(const MpsView<T>& mps, const SvdWork<T>
             ++sweep;
             break;
         }
+        mixed = still_mixed(mixed, done, N);
     }
     // column norms -> sig2 (FP64)
     {
@@ -741,6 +763,7 @@ __device__ void jacobi_core(cplx_t<T>* col, const int rc, const int R, const int
     int sweep = 0;
     converged = false;
     rotations = 0.0;
+    bool mixed = true;
     for (; sweep < max_sweeps; ++sweep) {
         int rot = 0;
         for (int r = 0; r < Nc - 1; ++r) {
@@ -776,7 +799,7 @@ __device__ void jacobi_core(cplx_t<T>* col, const int rc, const int R, const int
                     v3 += __shfl_xor_sync(0xffffffffu, v3, o);
                 }
                 T c, sn, er, ei;
-                if (ok && jacobi_rotation<T>(v0, v1, v2, v3, tol, tiny, c, sn, er, ei)) {
+                if (ok && jacobi_rotation<T>(v0, v1, v2, v3, tol, tiny, mixed, c, sn, er, ei)) {
 #pragma unroll
                     for (int k = 0; k < RPL; ++k) {
                         if (k >= rpl) break;
@@ -806,6 +829,7 @@ __device__ void jacobi_core(cplx_t<T>* col, const int rc, const int R, const int
             ++sweep;
             break;
         }
+        mixed = still_mixed(mixed, done, N);
     }
     sweeps = sweep;
     __syncthreads();
@@ -1244,7 +1268,8 @@ __device__ __forceinline__ bool bg_wait(uint64_t* bar, unsigned& ph, int* s_ok) 
 // One block pair: Gram, one Jacobi sweep on it, apply.  Returns false (on every thread) when
 // a copy did not complete within its time budget.
 template <typename T>
-__device__ bool bg_pair(const SvdWork<T>& wk, int R, int N, int I, int J, double tol, double tiny, double2* G,
+__device__ bool bg_pair(const SvdWork<T>& wk, int R, int N, int I, int J, double tol, double tiny, bool mixed,
+                        double2* G,
                         double2* Vm, cplx_t<T>* ch0, cplx_t<T>* ch1, uint64_t* bars, unsigned* phase, BgRot* prm,
                         int* s_rot, double* bytes, double* flops) {
     using V = cplx_t<T>;
@@ -1309,8 +1334,8 @@ __device__ bool bg_pair(const SvdWork<T>& wk, int R, int N, int I, int J, double
             t.p = p;
             t.q = q;
             const double2 gpq = G[p * BG_GS + q];
-            t.act = jacobi_rotation<double>(G[p * BG_GS + p].x, G[q * BG_GS + q].x, gpq.x, gpq.y, tol, tiny, t.c, t.s,
-                                            t.er, t.ei)
+            t.act = jacobi_rotation<double>(G[p * BG_GS + p].x, G[q * BG_GS + q].x, gpq.x, gpq.y, tol, tiny, mixed,
+                                            t.c, t.s, t.er, t.ei)
                         ? 1
                         : 0;
             prm[tid] = t;
@@ -1430,6 +1455,7 @@ __device__ void svd_bgj_body(const MpsView<T>& mps, const SvdWork<T>& wk, const 
     double flops = 0.0;
     int sweep = 0;
     bool converged = false;
+    bool mixed = true;
     for (; sweep < pp.max_sweeps; ++sweep) {
         if (tid == 0) s_rot[0] = 0;
         __syncthreads();
@@ -1437,7 +1463,7 @@ __device__ void svd_bgj_body(const MpsView<T>& mps, const SvdWork<T>& wk, const 
             for (int pr = 0; pr < P / 2; ++pr) {
                 int I, J;
                 tournament(P, r, pr, I, J);
-                if (!bg_pair<T>(wk, R, N, I, J, pp.tol, tiny, G, Vm, ch0, ch1, bars, phase, prm, s_rot, &bytes,
+                if (!bg_pair<T>(wk, R, N, I, J, pp.tol, tiny, mixed, G, Vm, ch0, ch1, bars, phase, prm, s_rot, &bytes,
                                 &flops)) {
                     // every thread leaves here together; wait (bounded) for the copies still in
                     // flight so that none lands in shared memory after the CTA has moved on
@@ -1458,6 +1484,7 @@ __device__ void svd_bgj_body(const MpsView<T>& mps, const SvdWork<T>& wk, const 
             ++sweep;
             break;
         }
+        mixed = still_mixed(mixed, done, N);
     }
     // column norms -> sig2 (FP64)
     for (int j = warp; j < N; j += NW) {
@@ -1652,6 +1679,7 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
     int sweep = 0;
     bool converged = false;
     bool fail = false;
+    bool mixed = true;
     for (; sweep < pp.max_sweeps && !fail; ++sweep) {
         if (tid == 0) s_rot = 0;
         __syncthreads();
@@ -1698,7 +1726,7 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
                     if (ip == 0) { x = BW - 1; y = t; }
                     else { x = (t + ip) % (BW - 1); y = (t - ip + (BW - 1)) % (BW - 1); }
                     const bool ok = (I * BW + x < N) && (I * BW + y < N);
-                    const int r1 = rotate_pair<T, G2>(ci + x * rc, ci + y * rc, ok, R, pp.tol, tiny, red, tid);
+                    const int r1 = rotate_pair<T, G2>(ci + x * rc, ci + y * rc, ok, R, pp.tol, tiny, mixed, red, tid);
                     if (r1 && (tid % G2) == 0) { ++rot; s_irot = 1; }
                     __syncthreads();
                 }
@@ -1748,7 +1776,7 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
                         v3 += __shfl_xor_sync(0xffffffffu, v3, o);
                     }
                     T c, sn, er, ei;
-                    if (ok && jacobi_rotation<T>(v0, v1, v2, v3, pp.tol, tiny, c, sn, er, ei)) {
+                    if (ok && jacobi_rotation<T>(v0, v1, v2, v3, pp.tol, tiny, mixed, c, sn, er, ei)) {
 #pragma unroll
                         for (int k = 0; k < RPL; ++k) {
                             const V x = xi[k], y = yj[k];
@@ -1806,6 +1834,7 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
             ++sweep;
             break;
         }
+        mixed = still_mixed(mixed, done, N);
     }
     if (fail) {
         // every thread leaves together; wait (bounded) for copies still in flight
