@@ -240,6 +240,14 @@ TESSERA_QA_API int tessera_qa_schedule_predict(tessera_qa_gnn* g, const tessera_
 /* Copies the calling thread's last error message into buf; returns its full length. */
 TESSERA_QA_API int tessera_qa_last_error(char* buf, size_t len);
 
+/* Fault injection for tests (no counterpart in the reference, which has no error path): after
+ * the next `after` device allocations made by the library (in any thread) succeed, the
+ * `count` following ones fail as if cudaMalloc had returned cudaErrorMemoryAllocation;
+ * count = 0 cancels what is left.  A call that meets the failure releases what it had
+ * allocated and returns TESSERA_QA_ECUDA (tessera_qa_anneal: NaN) with its outputs
+ * untouched.  Returns the number of injected failures that were still pending. */
+TESSERA_QA_API int tessera_qa_debug_fail_allocations(int after, int count);
+
 /* ---- sessions: device-resident anneal state (no host copies between calls) ---- */
 typedef struct tessera_qa_session tessera_qa_session;
 

@@ -5,6 +5,11 @@
 
 namespace tq {
 
+// Every device allocation of the library goes through here (engine.cu): cudaMalloc, except
+// that tessera_qa_debug_fail_allocations(after, count) makes chosen calls fail with
+// cudaErrorMemoryAllocation, so the out-of-memory paths can be tested without exhausting a GPU.
+cudaError_t device_alloc(void** p, size_t bytes);
+
 // ---------------------------------------------------------------------------------
 // Complex arithmetic on interleaved (re, im) pairs.  T = double (complex128 mode) or
 // float (complex64 mode).  Storage uses the CUDA vector types so loads are 16 / 8 byte

@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -42,6 +43,27 @@ struct ArgError : std::runtime_error {
 static thread_local std::string t_err;
 
 static void set_err(const std::string& s) { t_err = s; }
+
+// Allocation-failure injection (tessera_qa_debug_fail_allocations): allocations that still
+// succeed first, then allocations that fail.
+static std::mutex g_fail_mu;
+static int g_fail_after = 0, g_fail_count = 0;
+
+cudaError_t device_alloc(void** p, size_t bytes) {
+    {
+        std::lock_guard<std::mutex> lk(g_fail_mu);
+        if (g_fail_count > 0) {
+            if (g_fail_after > 0) {
+                --g_fail_after;
+            } else {
+                --g_fail_count;
+                *p = nullptr;
+                return cudaErrorMemoryAllocation;
+            }
+        }
+    }
+    return cudaMalloc(p, bytes);
+}
 void set_last_error(const std::string& msg) { t_err = msg; }
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -204,14 +226,20 @@ public:
         cap_ = (int)std::min<long long>(C.chi, full);
         if (cap_ < 1) cap_ = 1;
         ld_ = std::max(2 * cap_, (C.min_ld + 7) & ~7);
-        build_ops();
-        allocate();
-        TQ_CK(cudaEventCreate(&ev0_));
-        TQ_CK(cudaEventCreate(&ev1_));
-        upload_problem();
-        init_plus();
+        try {  // a failed allocation or CUDA call releases what was made before it
+            build_ops();
+            allocate();
+            TQ_CK(cudaEventCreate(&ev0_));
+            TQ_CK(cudaEventCreate(&ev1_));
+            upload_problem();
+            init_plus();
+        } catch (...) {
+            release();
+            throw;
+        }
     }
-    ~Engine() override {
+    ~Engine() override { release(); }
+    void release() noexcept {
         if (stream_) cudaStreamSynchronize(stream_);
         for (cudaEvent_t e : pool_) cudaEventDestroy(e);
         if (ev0_) cudaEventDestroy(ev0_);
@@ -220,6 +248,11 @@ public:
         if (res_base_) cudaFree(res_base_);
         if (obs_) cudaFree(obs_);
         if (stream_) cudaStreamDestroy(stream_);
+        pool_.clear();
+        ev0_ = ev1_ = nullptr;
+        base_ = res_base_ = nullptr;
+        obs_ = nullptr;
+        stream_ = nullptr;
     }
 
     cudaStream_t stream() const override { return stream_; }
@@ -353,7 +386,7 @@ public:
         const MpsView<T> M = mps();
         if (!obs_) {  // environments for the final observables, allocated on first use
             const size_t bytes = sizeof(V) * (size_t)cap_ * cap_ * obs_units_;
-            TQ_CK(cudaMalloc(&obs_, bytes));
+            TQ_CK(device_alloc((void**)&obs_, bytes));
             TQ_CK(cudaMemsetAsync(obs_, 0, sizeof(V), stream_));
             V one = mk<V>(1, 0);
             TQ_CK(cudaMemcpyAsync(obs_, &one, sizeof(V), cudaMemcpyHostToDevice, stream_));
@@ -398,13 +431,13 @@ public:
         const MpsView<T> M = mps();
         if (!obs_) {
             const size_t bytes = sizeof(V) * (size_t)cap_ * cap_ * obs_units_;
-            TQ_CK(cudaMalloc(&obs_, bytes));
+            TQ_CK(device_alloc((void**)&obs_, bytes));
             V one = mk<V>(1, 0);
             TQ_CK(cudaMemcpyAsync(obs_, &one, sizeof(V), cudaMemcpyHostToDevice, stream_));
         }
         launch_chain<T>(M, 1, obsR_, n_, obs_, xs_, bar_, stats_, cap_, stream_);
         int8_t* d = nullptr;
-        TQ_CK(cudaMalloc(&d, count * (size_t)n_));
+        TQ_CK(device_alloc((void**)&d, count * (size_t)n_));
         cudaError_t err = cudaSuccess;
         try {
             launch_sample<T>(M, obs_, (int)count, seed, d, stream_);
@@ -556,7 +589,7 @@ public:
         if (res_base_) return;
         const size_t a1 = align256(sizeof(InstTask<T>));
         const size_t a2 = a1 + align256(sizeof(GateOp) * std::max<size_t>(ops_.size(), 1));
-        TQ_CK(cudaMalloc(&res_base_, a2 + 256));
+        TQ_CK(device_alloc((void**)&res_base_, a2 + 256));
         res_inst_ = reinterpret_cast<InstTask<T>*>(res_base_);
         res_ops_ = reinterpret_cast<GateOp*>(res_base_ + a1);
         res_off_ = reinterpret_cast<int*>(res_base_ + a2);
@@ -704,7 +737,7 @@ private:
         add((void**)&amp2_, sizeof(double));
         add((void**)&spins_d_, n_);
         TQ_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-        TQ_CK(cudaMalloc(&base_, off));
+        TQ_CK(device_alloc((void**)&base_, off));
         for (auto& it : plan) *it.second = base_ + it.first;
         TQ_CK(cudaMemsetAsync(bar_, 0, sizeof(GridBar), stream_));
         TQ_CK(cudaMemsetAsync(stats_, 0, sizeof(RunStats), stream_));
@@ -864,6 +897,29 @@ template <typename T>
 class BatchEngine final : public BatchBase {
 public:
     BatchEngine(const std::vector<ProblemHost>& P, const std::vector<Config>& C) {
+        try {  // a failed allocation or CUDA call releases what was made before it
+            init(P, C);
+        } catch (...) {
+            release();
+            throw;
+        }
+    }
+    ~BatchEngine() override { release(); }
+    void release() noexcept {
+        if (st_) cudaStreamSynchronize(st_);
+        for (cudaEvent_t e : pool_) cudaEventDestroy(e);
+        if (e0_) cudaEventDestroy(e0_);
+        if (e1_) cudaEventDestroy(e1_);
+        if (base_) cudaFree(base_);
+        if (st_) cudaStreamDestroy(st_);
+        pool_.clear();
+        e0_ = e1_ = nullptr;
+        base_ = nullptr;
+        st_ = nullptr;
+    }
+
+private:
+    void init(const std::vector<ProblemHost>& P, const std::vector<Config>& C) {
         const int B = (int)P.size();
         int steps = 0;
         for (int b = 0; b < B; ++b) {
@@ -910,7 +966,7 @@ public:
         const size_t a3 = a2 + align256(sizeof(GateOp) * std::max<size_t>(ops_all.size(), 1));
         const size_t a4 = a3 + align256(sizeof(int) * (B + 1));
         const size_t bytes = a4 + align256(sizeof(int) * B);
-        TQ_CK(cudaMalloc(&base_, bytes));
+        TQ_CK(device_alloc((void**)&base_, bytes));
         step_ = reinterpret_cast<int*>(base_);
         work_ = reinterpret_cast<int*>(base_ + 64);
         insts_ = reinterpret_cast<InstTask<T>*>(base_ + a0);
@@ -930,14 +986,8 @@ public:
         theta_tc_ = C[0].theta_tc != 0;
         for (auto& e : eng_) TQ_CK(cudaStreamSynchronize(e->own_stream()));
     }
-    ~BatchEngine() override {
-        if (st_) cudaStreamSynchronize(st_);
-        for (cudaEvent_t e : pool_) cudaEventDestroy(e);
-        if (e0_) cudaEventDestroy(e0_);
-        if (e1_) cudaEventDestroy(e1_);
-        if (base_) cudaFree(base_);
-        if (st_) cudaStreamDestroy(st_);
-    }
+
+public:
     int size() const override { return (int)eng_.size(); }
     Engine<T>& at(int b) { return *eng_[b]; }
     void save(int b, void* buf, size_t bytes) override {
@@ -1122,6 +1172,43 @@ static void run_batch(const std::vector<ProblemHost>& P, const std::vector<Confi
     }
 }
 
+// Standalone SVD output: the U columns whose singular value lies under the Jacobi's noise floor
+// (8 sqrt(R) ulps of ||A||_F) carry rounding noise, not a resolved direction.  Each is replaced,
+// in descending order, by its part orthogonal to every column before it (classical Gram-Schmidt,
+// two passes), renormalised; a column with nothing left becomes zero.  U (R x k, row-major) is
+// then an isometry on its non-zero columns, as the reference's SVD makes its factor by
+// Gram-Schmidt (cuda/src/linalg.cpp:56-105).
+static void orthonormalise_subfloor(std::vector<double2>& U, int R, int k, const std::vector<double>& sig) {
+    double fro2 = 0.0;
+    for (int t = 0; t < k; ++t) fro2 += sig[t] * sig[t];
+    const double floor = 8.0 * std::sqrt((double)R) * 2.220446049250313e-16 * std::sqrt(fro2);
+    std::vector<double2> x(R);
+    for (int t = 0; t < k; ++t) {
+        if (sig[t] > floor) continue;
+        for (int i = 0; i < R; ++i) x[i] = U[(size_t)i * k + t];
+        double n0 = 0.0;
+        for (int i = 0; i < R; ++i) n0 += x[i].x * x[i].x + x[i].y * x[i].y;
+        for (int pass = 0; pass < 2; ++pass)
+            for (int q = 0; q < t; ++q) {
+                double re = 0.0, im = 0.0;  // u_q^H x
+                for (int i = 0; i < R; ++i) {
+                    const double2 u = U[(size_t)i * k + q];
+                    re += u.x * x[i].x + u.y * x[i].y;
+                    im += u.x * x[i].y - u.y * x[i].x;
+                }
+                for (int i = 0; i < R; ++i) {
+                    const double2 u = U[(size_t)i * k + q];
+                    x[i].x -= re * u.x - im * u.y;
+                    x[i].y -= re * u.y + im * u.x;
+                }
+            }
+        double n2 = 0.0;
+        for (int i = 0; i < R; ++i) n2 += x[i].x * x[i].x + x[i].y * x[i].y;
+        const double sc = (n0 > 0.0 && n2 > 1e-16 * n0) ? 1.0 / std::sqrt(n2) : 0.0;
+        for (int i = 0; i < R; ++i) U[(size_t)i * k + t] = make_double2(x[i].x * sc, x[i].y * sc);
+    }
+}
+
 }  // namespace tq
 
 using namespace tq;
@@ -1257,6 +1344,14 @@ double tessera_qa_anneal(const double* h, size_t n, const size_t* ei, const size
     return r.energy;
 }
 
+int tessera_qa_debug_fail_allocations(int after, int count) {
+    std::lock_guard<std::mutex> lk(g_fail_mu);
+    const int pending = g_fail_count;
+    g_fail_after = after < 0 ? 0 : after;
+    g_fail_count = count < 0 ? 0 : count;
+    return pending;
+}
+
 int tessera_qa_svd(const double* a, size_t rows, size_t cols, double* s, double* u, double* vh) {
     return guarded([&]() -> int {
         if (!a || !s) throw ArgError("a or s is NULL");
@@ -1289,6 +1384,7 @@ int tessera_qa_svd(const double* a, size_t rows, size_t cols, double* s, double*
                     U[(size_t)i * k + t] = make_double2(w.x / sig[t], w.y / sig[t]);
                 }
             }
+            orthonormalise_subfloor(U, R, k, sig);
             if (u) std::memcpy(u, U.data(), sizeof(double2) * U.size());
             if (vh) {
                 for (int t = 0; t < k; ++t)

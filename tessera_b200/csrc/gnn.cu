@@ -35,6 +35,8 @@
 
 namespace tq {
 
+cudaError_t device_alloc(void** p, size_t bytes);  // engine.cu: cudaMalloc with failure injection
+
 void set_last_error(const std::string& msg);
 
 #define GN_CK(x)                                                                                          \
@@ -425,12 +427,33 @@ public:
         Ly.K = K;
         Ly.F = 4;
         Ly.build();
+        try {  // a failed allocation or CUDA call releases what was made before it
+            init(seed);
+        } catch (...) {
+            release();
+            throw;
+        }
+    }
+    ~Gnn() { release(); }
+    void release() noexcept {
+        if (st) cudaStreamSynchronize(st);
+        if (arena) cudaFree(arena);
+        if (w) cudaFree(w);
+        if (wb) cudaFree(wb);
+        if (st) cudaStreamDestroy(st);
+        arena = nullptr;
+        w = nullptr;
+        wb = nullptr;
+        st = nullptr;
+    }
+    void init(unsigned long long seed) {
+        const int H = Ly.H, L = Ly.L, K = Ly.K;
         GN_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-        GN_CK(cudaMalloc(&w, sizeof(float) * Ly.total * 4));
+        GN_CK(device_alloc((void**)&w, sizeof(float) * Ly.total * 4));
         g = w + Ly.total;
         m1 = g + Ly.total;
         m2 = m1 + Ly.total;
-        GN_CK(cudaMalloc(&wb, sizeof(__nv_bfloat16) * Ly.total));
+        GN_CK(device_alloc((void**)&wb, sizeof(__nv_bfloat16) * Ly.total));
         // uniform fan-in initialisation from a seeded splitmix64 stream; biases zero
         std::vector<float> hw(Ly.total, 0.f);
         unsigned long long z = seed * 0x9E3779B97F4A7C15ull + 1;
@@ -456,13 +479,6 @@ public:
         fill(Ly.Wg2, (size_t)(K - 1) * H, H, 0.1);
         set_params(hw.data());
         GN_CK(cudaMemset(m1, 0, sizeof(float) * Ly.total * 2));
-    }
-    ~Gnn() {
-        if (st) cudaStreamSynchronize(st);
-        if (arena) cudaFree(arena);
-        if (w) cudaFree(w);
-        if (wb) cudaFree(wb);
-        if (st) cudaStreamDestroy(st);
     }
     void set_params(const float* host) {
         GN_CK(cudaMemcpy(w, host, sizeof(float) * Ly.total, cudaMemcpyHostToDevice));
@@ -631,7 +647,7 @@ private:
         add((void**)&da, sizeof(float) * (size_t)capN * H);
         add((void**)&dm, sizeof(float) * (size_t)capE * H);
         add((void**)&dz, sizeof(float) * capN);
-        GN_CK(cudaMalloc(&arena, off));
+        GN_CK(device_alloc((void**)&arena, off));
         for (auto& it : plan) *it.second = static_cast<char*>(arena) + it.first;
     }
 };
@@ -722,7 +738,7 @@ double tessera_qa_exact_ground(const double* h, size_t n, const size_t* ei, cons
         char* arena = nullptr;
         const size_t mm = std::max<size_t>(m, 1);
         const size_t bytes = 64 * 8 + 8 * n + 8 * mm + 8 * mm + 16 * blocks;
-        GN_CK(cudaMalloc(&arena, bytes));
+        GN_CK(device_alloc((void**)&arena, bytes));
         size_t off = 0;
         auto take = [&](size_t sz) {
             void* r = arena + off;

@@ -375,7 +375,7 @@ extern "C" int tessera_qa_sv_anneal(const tessera_qa_problem* P, double dt, int 
         const size_t rho_blocks = 1ull << passes.back().nrest;  // qubit-0 partials: one set per last-pass CTA
         const size_t o_bx = o_ent + al(8 * steps), o_rho = o_bx + al(8 * (size_t)grid);
         const size_t total = o_rho + al(32 * rho_blocks);
-        SV_CK(cudaMalloc(&arena, total));
+        SV_CK(device_alloc((void**)&arena, total));
         auto at = [&](size_t o) { return arena + o; };
         double2* psi = (double2*)at(o_psi);
         double *df = (double*)at(o_df), *dz = (double*)at(o_dz), *dh = (double*)at(o_h), *dw = (double*)at(o_w);
