@@ -102,26 +102,37 @@ extern "C" int tessera_qa_svd_noalloc(const double* d_a, size_t rows, size_t col
         NoAllocScratch* sc = noalloc_setup(dev);
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         const int R = (int)rows, N = (int)cols, k = R < N ? R : N;
+        // an error left pending by the caller's own earlier launches would otherwise be read
+        // back after ours and reported as this call's failure
+        (void)cudaGetLastError();
         // clear what must start at zero (the array keeps the previous call's contents)
         e = cudaMemsetAsync(&sc->bar, 0, sizeof(GridBar), s);
         if (e == cudaSuccess) e = cudaMemsetAsync(&sc->stats, 0, sizeof(RunStats), s);
         if (e != cudaSuccess) throw std::runtime_error(std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
-        k_noalloc_load<<<(R * N + 255) / 256, 256, 0, s>>>(reinterpret_cast<const double2*>(d_a), R, N, sc->W);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) throw std::runtime_error(std::string("launch: ") + cudaGetErrorString(e));
-        SvdWork<double> wk{nullptr, sc->W, kNoAllocMaxDim, sc->sig2, sc->sig, sc->perm,
-                           sc->counters, sc->scal, &sc->bar, &sc->stats};
-        MpsView<double> none{nullptr, nullptr, 0, 1, 0};
-        const int bw = N <= 64 ? 16 : 8;
-        const double tol = 1e-13;
-        launch_svd<double>(none, 0, k, tol, kNoAllocSweeps, wk, R, N, bw, s, R, N);
-        k_noalloc_store<<<(R * k + 255) / 256, 256, 0, s>>>(sc->W, sc->perm, sc->sig, R, k, d_s,
-                                                           reinterpret_cast<double2*>(d_u));
-        e = cudaGetLastError();
-        if (e != cudaSuccess) throw std::runtime_error(std::string("launch: ") + cudaGetErrorString(e));
+        // Once work is queued on the shared array, no error path returns before that work has
+        // finished: a next call could otherwise overlap it on the array.
+        try {
+            k_noalloc_load<<<(R * N + 255) / 256, 256, 0, s>>>(reinterpret_cast<const double2*>(d_a), R, N, sc->W);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) throw std::runtime_error(std::string("launch: ") + cudaGetErrorString(e));
+            SvdWork<double> wk{nullptr, sc->W, kNoAllocMaxDim, sc->sig2, sc->sig, sc->perm,
+                               sc->counters, sc->scal, &sc->bar, &sc->stats};
+            MpsView<double> none{nullptr, nullptr, 0, 1, 0};
+            const int bw = N <= 64 ? 16 : 8;
+            const double tol = 1e-13;
+            launch_svd<double>(none, 0, k, tol, kNoAllocSweeps, wk, R, N, bw, s, R, N);
+            k_noalloc_store<<<(R * k + 255) / 256, 256, 0, s>>>(sc->W, sc->perm, sc->sig, R, k, d_s,
+                                                               reinterpret_cast<double2*>(d_u));
+            e = cudaGetLastError();
+            if (e != cudaSuccess) throw std::runtime_error(std::string("launch: ") + cudaGetErrorString(e));
+        } catch (...) {
+            (void)cudaStreamSynchronize(s);
+            throw;
+        }
         int status = 0;
         e = cudaMemcpyAsync(&status, &sc->stats.status, sizeof(int), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        else (void)cudaStreamSynchronize(s);
         if (e != cudaSuccess) throw std::runtime_error(std::string("CUDA: ") + cudaGetErrorString(e));
         if (status) {
             set_last_error("kernel status bits set: " + std::to_string(status));

@@ -63,24 +63,26 @@ def test_svd_kernel_matches_reference_spectra(golden):
         assert np.linalg.norm(u @ np.diag(s) @ vh - A) < 1e-12 * np.linalg.norm(A) * max(A.shape)
 
 
-@pytest.mark.parametrize("shape", [(64, 64), (128, 96), (512, 512), (200, 300), (2048, 256), pytest.param(
-    (1024, 1024), marks=pytest.mark.xfail(reason="known limit: columns whose norm dips under the noise floor during "
-                                                 "the sweeps stay frozen; 29 singular values within 4.1x of the floor "
-                                                 "come back at it and the frozen columns' U/Vh are not orthogonal"))])
+@pytest.mark.parametrize("shape", [(64, 64), (128, 96), (512, 512), (200, 300), (2048, 256), (1024, 1024)])
 def test_svd_kernel_large_random(shape):
+    """Random unitary factors around a TEBD-like spectrum exp(-k/20).  Values above the
+    kernel's noise floor (8 sqrt(R) ulps of ||A||_F) are resolved to 1e-9 relative; those under
+    it come back under twice it.  At 1024 x 1024, 437 of the values lie under the floor, and
+    columns whose norm dips under it mid-sweep must still be orthogonalised against the resolved
+    ones (the early, mixed phase of the freeze rule), else values a few times the floor come
+    back at it and U loses orthogonality."""
     rng = np.random.Generator(np.random.PCG64(sum(shape)))
     A = rng.normal(size=shape) + 1j * rng.normal(size=shape)
-    # give it a TEBD-like decaying spectrum
     U, s, Vh = np.linalg.svd(A, full_matrices=False)
     s = np.exp(-np.arange(len(s)) / 20.0)
     A = (U * s) @ Vh
     u, sg, vh = ffi.svd(A)
-    # singular values below the kernel's noise floor, 8 sqrt(R) ulps of ||A||_F, are not
-    # resolved: those columns are frozen and report norms under the floor (at most 2.6e-13
-    # at 2048 rows here), while the constructed tail falls far below it
     floor = 8.0 * np.sqrt(max(shape)) * np.finfo(np.float64).eps * np.linalg.norm(A)
     assert np.allclose(sg, s, rtol=1e-9, atol=floor)
-    assert np.max(sg[s < floor]) <= floor if np.any(s < floor) else True
+    above = s > 4 * floor
+    assert np.max(np.abs(sg[above] - s[above]) / s[above]) < 1e-4
+    assert np.max(sg[s < floor]) <= 2 * floor if np.any(s < floor) else True
+    assert np.linalg.norm(u.conj().T @ u - np.eye(len(s))) < 1e-9
     assert np.linalg.norm(u @ np.diag(sg) @ vh - A) < 1e-11 * np.linalg.norm(A)
 
 
@@ -485,3 +487,131 @@ def test_ragged_three_regular_batch_with_mixed_chi():
         s1.close()
         assert e_batch == pytest.approx(e_single, rel=1e-3, abs=1e-4), (b, p.n, p.chi)
     sb.close()
+
+
+def test_exact_chi1024_n20_matches_statevector(oracle):
+    """Config 2b: the n=20 chain with couplings to distance 4 (J ~ U(-1, 1), h = 0) at exact
+    chi = 1024 = 2^(n/2), against the exact state vector in the engine's splitting, on the CPU
+    oracle and on the GPU (tessera_qa_sv_anneal).  The stated window is 12 Trotter steps at
+    fixed s = 0.5 with dt = 0.25: from |+>^n that saturates the central bond at 1024 (its
+    1024th Schmidt value is 3e-10 there, far above the noise floor), so the central updates
+    run the 1024 x 1024 theta through the cooperative column-pair SVD.  Fidelity within 1e-8,
+    <H> within 1e-8, the entropy trace within 1e-7, and the oracle's most probable pattern most
+    probable in the MPS too (h = 0: a pattern and its complement tie)."""
+    p = instances.chain_range(n=20, dmax=4, seed=2, T=1.0, dt=0.25, chi=1024)
+    sa = np.full(12, 0.5)
+    sb = np.full(12, 0.5)
+    inst = Instance(p.h, p.ei.astype(np.int32), p.ej.astype(np.int32), p.ew)
+    r = ffi.anneal(p.h, p.ei, p.ej, p.ew, sa, sb, dt=0.25, chi=1024, want_checkpoint=True)
+    assert r.status == 0 and r.max_trunc < 1e-20
+    assert r.max_bond == 1024
+    psi = ffi.sites_to_dense(ffi.checkpoint_to_sites(r.checkpoint)[1])
+    sv = oracle.sv_anneal(inst, sa, sb, 0.25, mode=1, want_state=True)
+    gsv = ffi.sv_anneal(p.h, p.ei, p.ej, p.ew, sa, sb, dt=0.25, mode=1, want_state=True)
+    for ref in (sv.state, gsv.state):
+        assert 1 - fidelity(psi, ref) < 1e-8
+    assert r.expected_energy == pytest.approx(sv.expected_energy, abs=1e-8)
+    assert np.max(np.abs(r.entropy - sv.entropy)) < 1e-7
+    p_mps, p_sv = np.abs(psi) ** 2 / np.vdot(psi, psi).real, np.abs(sv.state) ** 2
+    assert p_mps[int(np.argmax(p_sv))] == pytest.approx(p_mps.max(), rel=1e-9)
+
+
+def test_chain16_chi32_full_run_tracks_the_oracle():
+    """Config 1 end to end: the n=16 chain (J ~ N(0, 1), h ~ N(0, 0.5)), linear schedule, T=20,
+    dt=0.05, all 400 steps at chi=32 (truncating), against the oracle's accurate-SVD mode (the
+    reference's algorithm: keep rule, gauge, gate order), whose run is stored in
+    tests/golden/oracle_chain16_chi32.json (tests/golden/make_oracle_runs.py; two minutes of CPU).
+    Over 400 truncating steps the run amplifies rounding: moving the inputs by 4 ulps moves the
+    oracle's own <H> by about 7e-3.  So <H> and the entropy trace are held to ten times that
+    sensitivity plus 1e-6; the readout spins, which the perturbed runs all share, and the
+    readout energy are held exactly."""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "oracle_chain16_chi32.json")) as f:
+        g = json.load(f)
+    o, sens = g["out"], g["sensitivity"]
+    p = instances.chain_nn(n=16, seed=1, T=20.0, dt=0.05, chi=32)
+    assert p.steps == 400
+    r = ffi.anneal(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=32)
+    assert r.status == 0 and r.two_site_updates == o["updates"]
+    assert abs(r.expected_energy - o["expected_energy"]) <= 1e-6 * abs(o["expected_energy"]) + \
+        10 * sens["expected_energy"]
+    assert np.max(np.abs(r.entropy - np.array(o["entropy"]))) <= 1e-6 + 10 * sens["entropy"]
+    assert g["spins_stable"] and list(r.spins) == o["spins"]
+    assert r.energy == pytest.approx(o["energy"], abs=1e-9)
+
+
+def mps_fidelity(a, b):
+    """|<a|b>|^2 / (<a|a><b|b>) of two MPS given as site lists (Dl, 2, Dr), by left transfer
+    matrices rescaled at every site (the random MPS here are far from normalised)."""
+    def overlap(x, y):
+        e = np.ones((1, 1), np.complex128)
+        logs = 0.0
+        for A, B in zip(x, y):
+            e = sum(A[:, s, :].conj().T @ e @ B[:, s, :] for s in range(2))
+            m = np.max(np.abs(e))
+            e /= m
+            logs += np.log(m)
+        return e[0, 0], logs
+    ab, lab = overlap(a, b)
+    aa, laa = overlap(a, a)
+    bb, lbb = overlap(b, b)
+    return float(abs(ab) ** 2 / (aa.real * bb.real) * np.exp(2 * lab - laa - lbb))
+
+
+def left_norms(site):
+    """Norm of every left-bond slice A[a, :, :]: the kept singular values for a site that an
+    update last wrote as S Vh, and invariant under the SVD's phase freedom for every site."""
+    return np.sqrt(np.sum(np.abs(site) ** 2, axis=(1, 2)))
+
+
+@pytest.fixture(scope="module")
+def chi256_window(oracle):
+    """The headline update against the oracle: the bench's generator (chain with couplings to
+    distance 4, J ~ U(-1, 1), h = 0) at n = 40, a random MPS with every interior bond at
+    chi = 256, and three consecutive gate slots of the s = 0.5 step on interior bonds (swaps on
+    bonds 16, 15, 14): three truncating 512 x 512 updates.  The oracle applies the same slots
+    to the same MPS with the reference's update (keep rule, gauge A <- U, C <- S Vh) and an
+    accurate SVD."""
+    p = instances.chain_range(n=40, dmax=4, seed=2, T=50.0, dt=0.02, chi=256)
+    step = len(p.sa) // 2
+    bonds = []
+    for i, j in zip(p.ei, p.ej):
+        bonds += [k - 1 for k in range(int(j), int(i) + 1, -1)] + [int(i)] + [k for k in range(int(i) + 1, int(j))]
+    q0 = next(q for q, b in enumerate(bonds) if b >= 16)
+    s = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=256)
+    s.randomize(31)
+    start = ffi.checkpoint_to_sites(s.save())[1]
+    s.close()
+    inst = Instance(p.h, p.ei.astype(np.int32), p.ej.astype(np.int32), p.ew)
+    o_sites, st = oracle.apply_slots(inst, start, float(p.sb[step]), p.dt, 256, q0, q0 + 3)
+    return p, step, q0, start, o_sites, st
+
+
+@pytest.mark.parametrize("batched", [False, True])
+def test_truncating_chi256_updates_match_the_oracle(chi256_window, batched):
+    """Three truncating chi=256 updates (512 x 512 theta) through the cooperative single-instance
+    SVD and the batched block-row-cyclic SVD, against the oracle.  The cut is well conditioned
+    (relative gap at the cut above 1e-4 in every update), so two accurate SVDs differ there by
+    rounding over the gap: the states agree to infidelity 1e-12, the discarded-weight ratio to
+    1e-6 relative, and the kept singular values (left-slice norms of the sites last written as
+    S Vh, and the same norms of every other site) to 1e-10 relative."""
+    p, step, q0, start, o_sites, st = chi256_window
+    assert st["updates"] == 3 and st["min_cut_gap"] > 1e-4 and st["max_trunc"] > 1e-3
+    if batched:
+        s = ffi.Session.batch([p], chi=256)
+    else:
+        s = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=256)
+    s.randomize(31)
+    s.run_gates(step, q0, q0 + 3)
+    r = s.sync()
+    ck = s.save_instance(0) if batched else s.save()
+    s.close()
+    assert r.status == 0 and r.two_site_updates == 3
+    g_sites = ffi.checkpoint_to_sites(ck)[1]
+    assert [t.shape for t in g_sites] == [t.shape for t in o_sites]
+    assert 1 - mps_fidelity(g_sites, o_sites) < 1e-12
+    assert r.max_trunc == pytest.approx(st["max_trunc"], rel=1e-6)
+    for i, (g, o) in enumerate(zip(g_sites, o_sites)):
+        ng, no = left_norms(g), left_norms(o)
+        assert np.max(np.abs(ng - no) / no) < 1e-10, i
