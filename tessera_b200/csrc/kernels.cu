@@ -342,6 +342,22 @@ __device__ __forceinline__ bool jacobi_rotation(const double v0, const double v1
     return true;
 }
 
+// Per-lane partial sums of alpha = |x|^2, beta = |y|^2 and gamma = x^H y over the rows a lane
+// holds, for complex64: FP32 products summed in FP32 over the lane's rows (at most 16 in every
+// kernel here, relative error about 1e-6, under the complex64 convergence tolerance
+// 8 sqrt(R) eps_f32), so they run on the FP32 pipe; the lane sums are widened to FP64 before
+// the cross-lane sum, the noise-floor test and the FP64 convergence test.  complex128 keeps FP64
+// products and sums.
+struct LaneDotsF32 {
+    float a = 0.f, b = 0.f, gr = 0.f, gi = 0.f;
+    __device__ __forceinline__ void add(const float2 x, const float2 y) {
+        a = fmaf(x.x, x.x, fmaf(x.y, x.y, a));
+        b = fmaf(y.x, y.x, fmaf(y.y, y.y, b));
+        gr = fmaf(x.x, y.x, fmaf(x.y, y.y, gr));
+        gi = fmaf(x.x, y.y, fmaf(-x.y, y.x, gi));
+    }
+};
+
 // Rotate local columns p, q (shared memory) of a group; returns 1 if rotated.
 template <typename T, int G>
 __device__ __forceinline__ int rotate_pair(cplx_t<T>* cp, cplx_t<T>* cq, bool valid, int R, double tol,
@@ -350,12 +366,18 @@ __device__ __forceinline__ int rotate_pair(cplx_t<T>* cp, cplx_t<T>* cq, bool va
     const int lg = tid % G;
     double v[4] = {0.0, 0.0, 0.0, 0.0};
     if (valid) {
-        for (int r = lg; r < R; r += G) {
-            const V x = cp[r], y = cq[r];
-            v[0] += (double)x.x * x.x + (double)x.y * x.y;
-            v[1] += (double)y.x * y.x + (double)y.y * y.y;
-            v[2] += (double)x.x * y.x + (double)x.y * y.y;   // Re conj(x) y
-            v[3] += (double)x.x * y.y - (double)x.y * y.x;   // Im conj(x) y
+        if constexpr (sizeof(T) == 4) {
+            LaneDotsF32 d;
+            for (int r = lg; r < R; r += G) d.add(cp[r], cq[r]);
+            v[0] = d.a; v[1] = d.b; v[2] = d.gr; v[3] = d.gi;
+        } else {
+            for (int r = lg; r < R; r += G) {
+                const V x = cp[r], y = cq[r];
+                v[0] += (double)x.x * x.x + (double)x.y * x.y;
+                v[1] += (double)y.x * y.x + (double)y.y * y.y;
+                v[2] += (double)x.x * y.x + (double)x.y * y.y;   // Re conj(x) y
+                v[3] += (double)x.x * y.y - (double)x.y * y.x;   // Im conj(x) y
+            }
         }
     }
     group_reduce4<G>(v, red, tid);
@@ -644,13 +666,20 @@ __device__ __forceinline__ void svd_body(const MpsView<T>& mps, const SvdWork<T>
                             yj[k] = (row < R) ? cq[row] : czero<V>();
                         }
                         double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+                        if constexpr (sizeof(T) == 4) {
+                            LaneDotsF32 d;
 #pragma unroll
-                        for (int k = 0; k < RPL; ++k) {
-                            const V x = xi[k], y = yj[k];
-                            v0 += (double)x.x * x.x + (double)x.y * x.y;
-                            v1 += (double)y.x * y.x + (double)y.y * y.y;
-                            v2 += (double)x.x * y.x + (double)x.y * y.y;
-                            v3 += (double)x.x * y.y - (double)x.y * y.x;
+                            for (int k = 0; k < RPL; ++k) d.add(xi[k], yj[k]);
+                            v0 = d.a; v1 = d.b; v2 = d.gr; v3 = d.gi;
+                        } else {
+#pragma unroll
+                            for (int k = 0; k < RPL; ++k) {
+                                const V x = xi[k], y = yj[k];
+                                v0 += (double)x.x * x.x + (double)x.y * x.y;
+                                v1 += (double)y.x * y.x + (double)y.y * y.y;
+                                v2 += (double)x.x * y.x + (double)x.y * y.y;
+                                v3 += (double)x.x * y.y - (double)x.y * y.x;
+                            }
                         }
 #pragma unroll
                         for (int o = 16; o > 0; o >>= 1) {
@@ -783,13 +812,23 @@ __device__ void jacobi_core(cplx_t<T>* col, const int rc, const int R, const int
                     y[k] = in ? cq[row] : czero<V>();
                 }
                 double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+                if constexpr (sizeof(T) == 4) {
+                    LaneDotsF32 d;
 #pragma unroll
-                for (int k = 0; k < RPL; ++k) {
-                    if (k >= rpl) break;
-                    v0 += (double)x[k].x * x[k].x + (double)x[k].y * x[k].y;
-                    v1 += (double)y[k].x * y[k].x + (double)y[k].y * y[k].y;
-                    v2 += (double)x[k].x * y[k].x + (double)x[k].y * y[k].y;
-                    v3 += (double)x[k].x * y[k].y - (double)x[k].y * y[k].x;
+                    for (int k = 0; k < RPL; ++k) {
+                        if (k >= rpl) break;
+                        d.add(x[k], y[k]);
+                    }
+                    v0 = d.a; v1 = d.b; v2 = d.gr; v3 = d.gi;
+                } else {
+#pragma unroll
+                    for (int k = 0; k < RPL; ++k) {
+                        if (k >= rpl) break;
+                        v0 += (double)x[k].x * x[k].x + (double)x[k].y * x[k].y;
+                        v1 += (double)y[k].x * y[k].x + (double)y[k].y * y[k].y;
+                        v2 += (double)x[k].x * y[k].x + (double)x[k].y * y[k].y;
+                        v3 += (double)x[k].x * y[k].y - (double)x[k].y * y[k].x;
+                    }
                 }
 #pragma unroll
                 for (int o = LPP / 2; o > 0; o >>= 1) {
@@ -1609,6 +1648,11 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
     // this sweep's column order: descending norm (block position p holds column perm[p])
     __shared__ int perm[RC_MAXN];
     __shared__ int s_irot, s_jrot;
+    // cross rounds: column q of the J buffer has been through s_ver[q] rounds since the SVD
+    // began; warp w takes column (w + t) % BW in round t once its neighbour w + 1 has released
+    // it from round t - 1, so warps are not held in step by a CTA barrier per round
+    __shared__ int s_ver[BW];
+    __shared__ int s_fail;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int R = pp.R > 0 ? pp.R : 2 * mps.dims[pp.bond];
     const int N = pp.N > 0 ? pp.N : 2 * mps.dims[pp.bond + 2];
@@ -1657,6 +1701,9 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
         return;
     }
     for (int e = tid; e < N; e += NT) { cprev[e] = 1; ccur[e] = 1; }
+    if (tid < BW) s_ver[tid] = 0;
+    if (tid == 0) s_fail = 0;
+    int vbase = 0;  // rounds each J column has been through before the current J block
     double rots_total = 0.0;
     double pairs_checked = 0.0;
     double moved = 2.0 * nb;  // column blocks read or written (the norm passes: one read each)
@@ -1753,6 +1800,16 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
                     const int q = (warp + t) % BW;
                     const bool ok = vi && (J * BW + q < N);
                     V* cq = cb + q * rc;
+                    if (t > 0) {  // bounded wait for warp w + 1 to release column q from round t - 1
+                        if (lane == 0) {
+                            const volatile int* vq = &s_ver[q];
+                            unsigned spin = 0;
+                            while (*vq < vbase + t && !*(volatile int*)&s_fail)
+                                if (++spin > (1u << 24)) { s_fail = 1; break; }
+                        }
+                        __syncwarp();
+                        __threadfence_block();
+                    }
                     V yj[RPL];
 #pragma unroll
                     for (int k = 0; k < RPL; ++k) {
@@ -1760,13 +1817,20 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
                         yj[k] = (ok && row < R) ? cq[row] : czero<V>();
                     }
                     double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+                    if constexpr (sizeof(T) == 4) {
+                        LaneDotsF32 d;
 #pragma unroll
-                    for (int k = 0; k < RPL; ++k) {
-                        const V x = xi[k], y = yj[k];
-                        v0 += (double)x.x * x.x + (double)x.y * x.y;
-                        v1 += (double)y.x * y.x + (double)y.y * y.y;
-                        v2 += (double)x.x * y.x + (double)x.y * y.y;
-                        v3 += (double)x.x * y.y - (double)x.y * y.x;
+                        for (int k = 0; k < RPL; ++k) d.add(xi[k], yj[k]);
+                        v0 = d.a; v1 = d.b; v2 = d.gr; v3 = d.gi;
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < RPL; ++k) {
+                            const V x = xi[k], y = yj[k];
+                            v0 += (double)x.x * x.x + (double)x.y * x.y;
+                            v1 += (double)y.x * y.x + (double)y.y * y.y;
+                            v2 += (double)x.x * y.x + (double)x.y * y.y;
+                            v3 += (double)x.x * y.y - (double)x.y * y.x;
+                        }
                     }
 #pragma unroll
                     for (int o = 16; o > 0; o >>= 1) {
@@ -1792,8 +1856,14 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
                         }
                         if (lane == 0) { ++rot; s_jrot = 1; s_irot = 1; }
                     }
-                    __syncthreads();
+                    // release column q to warp w - 1 for round t + 1
+                    __syncwarp();
+                    __threadfence_block();
+                    if (lane == 0) *(volatile int*)&s_ver[q] = vbase + t + 1;
                 }
+                vbase += BW;
+                __syncthreads();
+                if (s_fail) { fail = true; break; }
                 // block J back to global memory when it changed; later bulk copies read it
                 if (s_jrot) {
                     moved += 1.0;
