@@ -237,6 +237,18 @@ TESSERA_QA_API int tessera_qa_gnn_apply_grads(tessera_qa_gnn* g, const float* gr
 TESSERA_QA_API int tessera_qa_schedule_predict(tessera_qa_gnn* g, const tessera_qa_problem* problems, size_t count,
                                                double* out_knots, double* out_bias);
 
+/* Best-of-restarts simulated annealing on the GPU for `count` instances (n <= 128 each): the
+ * best-known-energy scorer beyond brute force.  Restates rust/src/ising.rs:64-136 (sa_run,
+ * sa_solve): random start, geometric temperatures t0 -> t_end over `sweeps` Metropolis sweeps in
+ * spin order, lowest final energy over `restarts` runs (first on ties).  The uniforms come from a
+ * counter-based splitmix64 stream keyed by (seed, instance, restart, sweep, spin) instead of the
+ * reference's StdRng.  Writes each instance's best spins (concatenated, n per instance, +-1) and
+ * energy.  The reference's own use is restarts 40, sweeps 400, t0 5.0, t_end 0.01
+ * (rust/src/bin/bench.rs:46). */
+TESSERA_QA_API int tessera_qa_sa_solve(const tessera_qa_problem* problems, size_t count, size_t restarts,
+                                       size_t sweeps, double t0, double t_end, uint64_t seed,
+                                       int8_t* out_spins, double* out_energy);
+
 /* Copies the calling thread's last error message into buf; returns its full length. */
 TESSERA_QA_API int tessera_qa_last_error(char* buf, size_t len);
 

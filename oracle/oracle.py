@@ -101,6 +101,9 @@ class Oracle:
                                          C.c_double, C.c_int, _i8p, _i8p, _dp, _dp, _dp, _dp, _dp]
         L.orc_exact_ground.argtypes = [_dp, C.c_int, _ip, _ip, _dp, C.c_int, _i8p]
         L.orc_exact_ground.restype = C.c_double
+        L.orc_sa_solve.argtypes = [_dp, C.c_int, _ip, _ip, _dp, C.c_int, C.c_int, C.c_int, C.c_double,
+                                   C.c_double, C.c_uint64, C.c_uint64, _i8p]
+        L.orc_sa_solve.restype = C.c_double
         L.orc_svd.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp]
         L.orc_mps_apply_slots.argtypes = [C.c_int, _ip, _dp, _ip, _ip, _dp, C.c_int, C.c_double, C.c_double,
                                           C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _ip, _dp,
@@ -185,6 +188,16 @@ class Oracle:
         s = np.zeros(len(h), np.int8)
         e = self.lib.orc_exact_ground(_ptr(h, _dp), len(h), _ptr(ei, _ip), _ptr(ej, _ip),
                                       _ptr(ew, _dp), len(ew), _ptr(s, _i8p))
+        return s, float(e)
+
+    def sa_solve(self, inst: Instance, restarts: int, sweeps: int, t0: float = 5.0, t_end: float = 0.01,
+                 seed: int = 0, index: int = 0):
+        """Best-of-restarts simulated annealing (rust/src/ising.rs:64-136) with the library's
+        counter-based uniforms; `index` is the instance's position in a tessera_qa_sa_solve batch."""
+        h, ei, ej, ew = _d(inst.h), _i(inst.ei), _i(inst.ej), _d(inst.ew)
+        s = np.zeros(len(h), np.int8)
+        e = self.lib.orc_sa_solve(_ptr(h, _dp), len(h), _ptr(ei, _ip), _ptr(ej, _ip), _ptr(ew, _dp), len(ew),
+                                  restarts, sweeps, t0, t_end, seed, index, _ptr(s, _i8p))
         return s, float(e)
 
     def svd(self, a: np.ndarray):

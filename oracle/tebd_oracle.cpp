@@ -734,6 +734,53 @@ double orc_exact_ground(const double* h, int n, const int* ei, const int* ej, co
     return best;
 }
 
+// Best-of-restarts simulated annealing (rust/src/ising.rs:64-136: sa_run, simulated_annealing,
+// sa_solve): random start; sweep k at t0 (t_end/t0)^(k/(max(sweeps,2)-1)); spins 0..n-1 in order,
+// flip when dE = 2 s_i (h_i + sum_j J_ij s_j) < 0 or u < exp(-dE/t); energy of the final pattern
+// (Ising::energy, rust/src/ising.rs:23-32); the lowest over restarts, the first on ties.  The
+// uniforms follow the library's counter-based stream (splitmix64's finaliser over the counter
+// (seed, instance, restart, sweep, spin); the start pattern uses sweep = sweeps), so the GPU
+// solver can be checked against this one draw for draw; the reference's StdRng stream is not
+// reproducible without its Rust crate.  Fields are summed over each spin's neighbours in the
+// order the edge list lists them.
+static double sa_u(uint64_t seed, uint64_t inst, uint64_t r, uint64_t k, uint64_t i, uint64_t sweeps, uint64_t n) {
+    uint64_t x = seed + 0x9E3779B97F4A7C15ull * ((((inst * 0x100000001B3ull + r) * (sweeps + 1) + k) * n + i) + 1);
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    x ^= x >> 31;
+    return (double)(x >> 11) * (1.0 / 9007199254740992.0);
+}
+
+double orc_sa_solve(const double* h, int n, const int* ei, const int* ej, const double* ew, int m,
+                    int restarts, int sweeps, double t0, double t_end, uint64_t seed, uint64_t inst,
+                    int8_t* out_spins) {
+    std::vector<std::vector<std::pair<int, double>>> adj(n);
+    for (int e = 0; e < m; ++e) {
+        if (ei[e] == ej[e]) continue;
+        adj[ei[e]].push_back({ej[e], ew[e]});
+        adj[ej[e]].push_back({ei[e], ew[e]});
+    }
+    const double den = (double)((sweeps < 2 ? 2 : sweeps) - 1);
+    double best = INFINITY;
+    std::vector<int8_t> s(n), bs(n, 1);
+    for (int r = 0; r < restarts; ++r) {
+        for (int i = 0; i < n; ++i) s[i] = sa_u(seed, inst, r, sweeps, i, sweeps, n) < 0.5 ? -1 : 1;
+        for (int k = 0; k < sweeps; ++k) {
+            const double t = t0 * std::pow(t_end / t0, (double)k / den);
+            for (int i = 0; i < n; ++i) {
+                double f = h[i];
+                for (auto& pr : adj[i]) f += s[pr.first] < 0 ? -pr.second : pr.second;
+                const double de = 2.0 * (s[i] < 0 ? -f : f);
+                if (de < 0.0 || sa_u(seed, inst, r, k, i, sweeps, n) < std::exp(-de / t)) s[i] = -s[i];
+            }
+        }
+        const double e = ising_energy(s, h, n, ei, ej, ew, m);
+        if (e < best) { best = e; bs = s; }
+    }
+    if (out_spins) for (int i = 0; i < n; ++i) out_spins[i] = bs[i];
+    return best;
+}
+
 // Exact state-vector anneal.  mode 0 restates rust/src/quantum.rs:63-112 exactly
 // (diag phase b dt/2, Prod exp(+i a dt X), diag phase b dt/2; basis bit set <-> +1);
 // mode 1 uses the MPS engine's splitting (exp(-i dt/2 g_i) per site, ZZ phases for dt,

@@ -90,6 +90,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.tessera_qa_svd_noalloc.restype = C.c_int
         L.tessera_qa_last_error.argtypes = [C.c_char_p, C.c_size_t]
         L.tessera_qa_last_error.restype = C.c_int
+        L.tessera_qa_sa_solve.argtypes = [C.POINTER(Problem), C.c_size_t, C.c_size_t, C.c_size_t, C.c_double,
+                                          C.c_double, C.c_uint64, c_int8_p, c_double_p]
+        L.tessera_qa_sa_solve.restype = C.c_int
         L.tessera_qa_debug_fail_allocations.argtypes = [C.c_int, C.c_int]
         L.tessera_qa_debug_fail_allocations.restype = C.c_int
         L.tessera_qa_session_create.argtypes = [C.POINTER(Problem), C.POINTER(Config)]

@@ -224,6 +224,28 @@ def svd(a: np.ndarray):
     return u, s, vh
 
 
+def sa_solve(problems, restarts: int = 256, sweeps: int = 2000, t0: float = 5.0, t_end: float = 0.01,
+             seed: int = 0):
+    """Best-of-restarts simulated annealing on the GPU (tessera_qa_sa_solve) for a list of
+    problems (objects with h, ei, ej, ew): returns (energies, [spins per problem])."""
+    L = _lib.load()
+    arr = (_lib.Problem * len(problems))()
+    keep = []
+    for b, p in enumerate(problems):
+        P, k = problem_struct(p.h, p.ei, p.ej, p.ew, np.zeros(0), np.zeros(0))
+        arr[b] = P
+        keep.append(k)
+    ns = [len(p.h) for p in problems]
+    spins = np.zeros(sum(ns), np.int8)
+    en = np.zeros(len(problems))
+    rc = L.tessera_qa_sa_solve(arr, len(problems), restarts, sweeps, t0, t_end, seed,
+                               spins.ctypes.data_as(_lib.c_int8_p), en.ctypes.data_as(_lib.c_double_p))
+    if rc != 0:
+        raise _lib.EngineError(rc, _lib.last_error())
+    off = np.cumsum([0] + ns)
+    return en, [spins[off[b]:off[b + 1]].copy() for b in range(len(problems))]
+
+
 def checkpoint_to_sites(buf: bytes):
     """Decode a checkpoint into (dims, [site tensors (Dl, 2, Dr) complex128])."""
     raw = np.frombuffer(buf, dtype=np.uint8)

@@ -192,3 +192,16 @@ def test_null_handles_and_structs_are_rejected_without_a_gpu():
     assert L.tessera_qa_gnn_param_count(None) == 0
     L.tessera_qa_session_destroy(None)
     L.tessera_qa_gnn_destroy(None)
+
+
+def test_sa_solver_rejects_invalid_input_without_a_gpu():
+    from tessera_b200 import instances
+    p = instances.dense_er(8, 1, T=1.0, dt=0.1, chi=8)
+    for kw in ({"restarts": 0}, {"sweeps": 0}, {"t0": 0.0}, {"t_end": float("nan")}):
+        with pytest.raises(_lib.EngineError) as e:
+            ffi.sa_solve([p], **kw)
+        assert e.value.code == _lib.EINVAL, kw
+    big = instances.chain_range(n=130, dmax=1, seed=1, T=1.0, dt=0.1, chi=8)
+    with pytest.raises(_lib.EngineError) as e:
+        ffi.sa_solve([big])
+    assert e.value.code == _lib.EINVAL and "128" in str(e.value)

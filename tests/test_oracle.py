@@ -222,3 +222,39 @@ def test_apply_slots_equals_zz_phases_on_the_dense_state(oracle):
     part, st2 = oracle.apply_slots(inst, sites, B, dt, 8, 2, 5)
     assert st2["updates"] == 3
     assert all(np.array_equal(part[i], sites[i]) for i in range(4, n))
+
+
+def _rand_instance(n, p, rng):
+    """rust/src/ising.rs:143-153 (random_instance): h ~ U(-1, 1), each pair an edge with
+    probability p, J ~ U(-1, 1) -- drawn here from numpy's PCG64 (StdRng is not reproducible)."""
+    h = rng.uniform(-1, 1, n)
+    ei, ej, ew = [], [], []
+    for i in range(n):
+        for k in range(i + 1, n):
+            if rng.random() < p:
+                ei.append(i); ej.append(k); ew.append(rng.uniform(-1, 1))
+    return Instance(h, np.array(ei, np.int32), np.array(ej, np.int32), np.array(ew))
+
+
+def test_oracle_sa_reaches_exact_ground_state_on_small_instances(oracle):
+    """The reference's own SA claim (rust/src/ising.rs:156-174): best of 40 restarts x 400 sweeps,
+    t0 = 5, t_end = 0.01, reaches the exact ground energy on at least 19 of 20 random n=12, p=0.5
+    instances; and its returned energy is the energy of its returned pattern."""
+    rng = np.random.Generator(np.random.PCG64(1))
+    hits = 0
+    for k in range(20):
+        m = _rand_instance(12, 0.5, rng)
+        _, e_exact = oracle.exact_ground(m)
+        s, e_sa = oracle.sa_solve(m, 40, 400, seed=1, index=k)
+        assert e_sa == pytest.approx(m.energy(s), abs=1e-12)
+        hits += abs(e_sa - e_exact) < 1e-6
+    assert hits >= 19
+
+
+def test_oracle_single_sa_run_beats_a_random_pattern(oracle):
+    """rust/src/ising.rs:176-183: one run of 400 sweeps (t0 = 3) ends below a random pattern."""
+    rng = np.random.Generator(np.random.PCG64(2))
+    m = _rand_instance(16, 0.5, rng)
+    rand_s = rng.choice([-1, 1], 16)
+    _, e = oracle.sa_solve(m, 1, 400, t0=3.0, seed=2)
+    assert e < m.energy(rand_s)
