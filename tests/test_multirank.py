@@ -117,3 +117,67 @@ def test_data_parallel_training_matches_one_process():
             net.apply_grads(g.astype(np.float64), lr=0.1)
     assert np.allclose(out[0][1], net.theta, rtol=1e-6, atol=1e-6)
     assert learned.spin_targets([np.ones(2)]).tolist() == [1.0, 1.0]
+
+
+def _ragged_problems():
+    from tessera_b200 import instances
+    probs = [instances.dense_er(4 + (7 * k) % 13, 70 + k, T=0.5 + 0.1 * (k % 4), dt=0.1, chi=8 << (k % 3))
+             for k in range(37)]
+    probs += instances.batch_3_regular(count=8, T=0.2, dt=0.05, nmin=32, nmax=40)
+    return probs
+
+
+def _stub_runner(probs, fail=False):
+    """Stands in for ffi.anneal_batch on CPU: one record per problem, computed from it alone."""
+    if fail:
+        raise RuntimeError("injected failure")
+    from tessera_b200 import shard
+    return [{"name": p.name, "n": p.n, "cost": shard.instance_cost(p)} for p in probs]
+
+
+def _ragged_rank(rank, world, port, q):
+    import torch.distributed as dist
+
+    from tessera_b200 import shard
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    probs = _ragged_problems()
+    out = shard.run_ragged(probs, runner=_stub_runner)
+    try:
+        shard.run_ragged(probs, runner=lambda ps: _stub_runner(ps, fail=(rank == 1)))
+        failed = None
+    except shard.ShardError as e:
+        failed = e.failures
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((rank, out, failed))
+
+
+def test_ragged_batch_partitioned_by_cost_and_gathered():
+    """tessera_b200.shard on two gloo ranks: a ragged batch (dense instances of n 4..16 with bond
+    caps 8..32 and 3-regular instances of n 32..40, deliberately uneven costs) is partitioned by
+    estimated cost with the largest rank load within 15% of the best any partition can reach
+    (the mean load or the largest instance, whichever is larger); the gathered records, on
+    every rank, equal a one-process run in the original order; and a failure on one rank raises
+    on both, naming that rank."""
+    from tessera_b200 import shard
+    probs = _ragged_problems()
+    costs = [shard.instance_cost(p) for p in probs]
+    parts = shard.partition(costs, 2)
+    assert sorted(i for p in parts for i in p) == list(range(len(probs)))
+    assert max(costs) / min(costs) > 100  # the batch really is ragged
+    assert shard.imbalance(costs, parts) < 1.15
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_ragged_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    out = sorted((q.get(timeout=180) for _ in ps), key=lambda t: t[0])
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    local = shard.run_ragged(probs, runner=_stub_runner)  # no process group: one process
+    for rank, recs, failed in out:
+        assert recs == local
+        assert failed is not None and set(failed) == {1} and "injected failure" in failed[1]
