@@ -43,7 +43,7 @@ def _gpu_name() -> str:
 def candidates(precision: str):
     out = [(8, False), (4, False), (32, False)]
     if precision == "c64":
-        out.append((8, True))
+        out += [(16, False), (8, True)]
     return out
 
 

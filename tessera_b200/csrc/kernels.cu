@@ -2514,6 +2514,17 @@ static void svd_batch_bw(const InstTask<T>* insts, const UpdRef* refs, int nref,
     TQ_CHECK(cudaGetLastError());
 }
 
+// complex64 at 512 rows: blocks of 16 columns (512 threads, 16 warps); a complex128 column pair
+// of 512 rows does not fit in the registers that 16 warps leave each thread
+template <typename T>
+static bool svd_batch_wide(const InstTask<T>* insts, const UpdRef* refs, int nref, int rows_cap, cudaStream_t s) {
+    if constexpr (sizeof(T) == 4) {
+        svd_batch_bw<T, 16, 16>(insts, refs, nref, rows_cap, s);
+        return true;
+    }
+    return false;
+}
+
 template <typename T>
 void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref, int d_ub, int rows_ub,
                          int block_w, cudaStream_t s, cudaEvent_t svd_begin, cudaEvent_t svd_end, bool theta_tc) {
@@ -2535,7 +2546,7 @@ void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref,
     while (32 * rpl < rows_cap) rpl <<= 1;
     if (rpl > 16 && block_w != BG_B) throw std::runtime_error("the column-pair batched SVD supports at most 512 rows");
     int bw = block_w < 4 ? 4 : block_w;
-    if (rpl == 16 && bw > 8) bw = 8;
+    if (rpl == 16 && bw > 8 && !(sizeof(T) == 4 && bw == 16)) bw = 8;
     if (svd_begin) TQ_CHECK(cudaEventRecord(svd_begin, s));
     SvdParams rp{};
     rp.rows_cap = rows_cap;
@@ -2546,6 +2557,7 @@ void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref,
     if (res_dispatch<T>(nullptr, nullptr, rp, insts, refs, nref, s)) {
     } else if (block_w == BG_B) {
         bgj_launch<T>(nullptr, nullptr, nullptr, insts, refs, nref, s);
+    } else if (bw == 16 && rpl == 16 && svd_batch_wide<T>(insts, refs, nref, rows_cap, s)) {
     } else {
 #define TQ_RB(B, RP) \
     if (bw == B && rpl == RP) { svd_batch_bw<T, B, RP>(insts, refs, nref, rows_cap, s); } else
