@@ -10,7 +10,7 @@ from tessera_b200 import autotune, instances
 def test_tune_picks_fastest_and_caches(tmp_path, monkeypatch):
     probs = [instances.chain_range(n=40, dmax=2, seed=s, T=1.0, dt=0.05, chi=64) for s in (1, 2)]
     calls = []
-    times = {(8, False): 3.0, (4, False): 2.0, (32, False): None, (8, True): 2.5}
+    times = {(8, False): 3.0, (4, False): 2.0, (32, False): None, (16, False): 2.2, (8, True): 2.5}
 
     def fake(problems, chi, precision, block, tc, q0, gates, seed=1234):
         calls.append((block, tc, q0, gates))
