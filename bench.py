@@ -68,6 +68,17 @@ def parse():
     ap.add_argument("--no-solves", action="store_true", help="skip the solves/s (chosen vs plain) measurement")
     ap.add_argument("--solve-instances", type=int, default=296, help="held-out instances for solves/s")
     ap.add_argument("--solve-T", type=float, default=10.0, help="anneal time of the solves/s workload")
+    ap.add_argument("--solve-dt", type=float, default=0.1)
+    ap.add_argument("--solve-chi", type=int, default=32)
+    ap.add_argument("--solve-nmin", type=int, default=12, help="held-out instances: n from nmin to nmax")
+    ap.add_argument("--solve-nmax", type=int, default=14)
+    ap.add_argument("--solve-train", type=int, default=160, help="training instances, n from 8 to --solve-train-nmax")
+    ap.add_argument("--solve-train-nmax", type=int, default=12)
+    ap.add_argument("--solve-train-T", type=float, default=None, help="anneal time of the labels (default --solve-T)")
+    ap.add_argument("--plain-sample", type=int, default=8, help="plain instances timed one call each")
+    ap.add_argument("--plain-steps", type=int, default=None,
+                    help="time the plain calls on the first k schedule steps and scale to the full schedule")
+    ap.add_argument("--solves-only", action="store_true", help="run only the solves/s study; print its JSON")
     ap.add_argument("--profile-run", action="store_true",
                     help="one untimed step only (for ncu); prints no bench line")
     ap.add_argument("--profile-sv", action="store_true",
@@ -309,40 +320,49 @@ def solves(args):
     """Second half of the metric: solves/s at <= 1% energy gap, chosen vs plain.
 
     Dense Erdos-Renyi instances (p = 0.5, J ~ U(-1,1), h ~ U(-0.2,0.2)).  The schedule GNN is
-    trained here, on the GPU, from labels the engine itself generates: 160 training instances
-    n in [8, 12], each annealed under 16 candidate schedules (batched, complex64) and scored by
-    the exact ground energy.  Then on `--solve-instances` held-out instances n in [12, 14]:
-    chosen = learned knots + warm-start bias, batched complex64, with the linear-schedule
-    fallback judged by the engine's own final energy; plain = linear schedule, complex128, one
-    instance per call (timed on 8 instances; energies of all instances from the bit-identical
-    batched complex128 run).  T = --solve-T, dt = 0.1, chi = 32."""
+    trained here, on the GPU, from labels the engine itself generates: --solve-train training
+    instances, n from 8 to --solve-train-nmax, each annealed under 16 candidate schedules
+    (batched, complex64) and scored by the exact ground energy.  Then on --solve-instances
+    held-out instances, n from --solve-nmin to --solve-nmax: chosen = learned knots + warm-start
+    bias, batched complex64, with the linear-schedule fallback judged by the engine's own final
+    energy; plain = linear schedule, complex128, one instance per call (timed on --plain-sample
+    instances, over the first --plain-steps steps when given and scaled to the whole schedule;
+    energies of all instances from the bit-identical batched complex128 run).  Scores are
+    against the exact ground energy for n <= 24, else against the best of a large simulated-
+    annealing budget on the GPU.  The learned and the linear runs are also reported each on
+    their own (no fallback): the network's gain over the method without it."""
     from tessera_b200 import instances, learned
-    cfg = learned.LearnConfig(T=args.solve_T, dt=0.1, chi=32, precision="c64")
-    train = [instances.dense_er(n, 1000 + i, T=1.0) for i, n in enumerate(list(range(8, 13)) * 32)]
+    cfg = learned.LearnConfig(T=args.solve_T, dt=args.solve_dt, chi=args.solve_chi, precision="c64")
+    tcfg = learned.LearnConfig(T=args.solve_train_T or args.solve_T, dt=args.solve_dt, chi=min(args.solve_chi, 32),
+                               precision="c64")
+    ns = list(range(8, args.solve_train_nmax + 1))
+    train = [instances.dense_er(n, 1000 + i, T=1.0) for i, n in
+             enumerate((ns * (args.solve_train // len(ns) + 1))[:args.solve_train])]
+    hs = list(range(args.solve_nmin, args.solve_nmax + 1))
     held = [instances.dense_er(n, 50000 + i, T=1.0) for i, n in
-            enumerate(([12, 13, 14] * (args.solve_instances // 3 + 1))[:args.solve_instances])]
+            enumerate((hs * (args.solve_instances // len(hs) + 1))[:args.solve_instances])]
     t0 = time.perf_counter()
-    tk, _, gs, gaps = learned.label(train, cfg, learned.candidates(count=16))
+    tk, _, gs, gaps = learned.label(train, tcfg, learned.candidates(count=16))
     t_label = time.perf_counter() - t0
     net = learned.ScheduleGNN(seed=1)
     t0 = time.perf_counter()
     losses = learned.train(net, train, tk, gs, epochs=100, batch=32, lr=2e-3)
     t_train = time.perf_counter() - t0
-    ev = learned.evaluate(net, held, cfg, plain_sample=8)
+    ev = learned.evaluate(net, held, cfg, plain_sample=args.plain_sample, plain_steps=args.plain_steps)
     net.close()
-    return {"metric": "solves/s at <=1% energy gap, chosen vs plain", "unit": "solves/s",
-            "chosen": ev["chosen_solves_per_s"], "plain": ev["plain_solves_per_s"],
-            "ratio": ev["chosen_solves_per_s"] / ev["plain_solves_per_s"] if ev["plain_solves_per_s"] else None,
-            "instances": ev["instances"], "chosen_solved": ev["chosen_solved"], "plain_solved": ev["plain_solved"],
-            "chosen_seconds": ev["chosen_seconds"], "plain_seconds": ev["plain_seconds"],
-            "plain_timed_instances": ev["plain_timed_instances"], "learned_kept": ev["learned_kept"],
-            "chosen_mean_gap": ev["chosen_mean_gap"], "plain_mean_gap": ev["plain_mean_gap"],
-            "train": {"instances": len(train), "candidates": 16, "label_seconds": t_label,
-                      "train_seconds": t_train, "loss_first": losses[0], "loss_last": losses[-1],
-                      "best_candidate_solved": int((gaps.min(axis=1) <= 0.01).sum()),
-                      "linear_solved": int((gaps[:, 0] <= 0.01).sum())},
-            "workload": f"dense ER p=0.5, train n 8..12, held-out n 12..14, T={cfg.T}, dt={cfg.dt}, chi={cfg.chi}; "
-                        "reduced from the full learned-schedule study (20k train n 8..20, 1024 eval n 24..48, chi=128, T=30)"}
+    out = {"metric": "solves/s at <=1% energy gap, chosen vs plain", "unit": "solves/s",
+           "chosen": ev["chosen_solves_per_s"], "plain": ev["plain_solves_per_s"],
+           "ratio": ev["chosen_solves_per_s"] / ev["plain_solves_per_s"] if ev["plain_solves_per_s"] else None}
+    out.update({k: v for k, v in ev.items() if k not in ("chosen_solves_per_s", "plain_solves_per_s")})
+    out["train"] = {"instances": len(train), "n": [8, args.solve_train_nmax], "candidates": 16, "T": tcfg.T,
+                    "chi": tcfg.chi, "label_seconds": t_label, "train_seconds": t_train, "loss_first": losses[0],
+                    "loss_last": losses[-1], "best_candidate_solved": int((gaps.min(axis=1) <= 0.01).sum()),
+                    "linear_solved": int((gaps[:, 0] <= 0.01).sum())}
+    out["workload"] = (f"dense ER p=0.5, train {len(train)} instances n 8..{args.solve_train_nmax} (labels at "
+                       f"T={tcfg.T}, chi={tcfg.chi}), held-out {len(held)} instances n {args.solve_nmin}.."
+                       f"{args.solve_nmax}, T={cfg.T}, dt={cfg.dt}, chi={cfg.chi}; the full learned-schedule study "
+                       "is 20k train n 8..20 and 1024 eval n 24..48 at chi=128, T=30")
+    return out
 
 
 def profile_anneal():
@@ -375,6 +395,10 @@ def main():
         return
     if args.profile_sv:
         profile_sv()
+        return
+    if args.solves_only:
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps({"solves": solves(args)}))
         return
     import numpy as np
     import torch
