@@ -297,9 +297,16 @@ __device__ __forceinline__ bool pair_live(const double v0, const double v1, cons
     return mixed ? (fmax(v0, v1) > tiny && lo > 1e-6 * tiny) : lo > tiny;
 }
 
-// Whether the next sweep stays in the mixed phase, from this sweep's rotation count.
-__device__ __forceinline__ bool still_mixed(const bool mixed, const double rotated, const int N) {
-    return mixed && rotated >= 0.05 * (double)N * (double)(N - 1);
+// Whether the next sweep stays in the mixed phase: this sweep rotated at least 10% of the pairs,
+// and the phase has not yet lasted 4 + 2 log2(N) sweeps.  The cap bounds the phase on the rare
+// theta where a few mixed pairs keep rotating by rounding (seen on small exact-chi theta: the
+// count then stays above 10% of a handful of pairs and the sweeps never settle); the late rule
+// converges from there.  Random 1024-column matrices leave the phase after 17 sweeps, under
+// the cap of 24.
+__device__ __forceinline__ bool still_mixed(const bool mixed, const double rotated, const int N, const int sweep) {
+    int lg = 0;
+    while ((1 << lg) < N) ++lg;
+    return mixed && rotated >= 0.05 * (double)N * (double)(N - 1) && sweep + 1 < 4 + 2 * lg;
 }
 
 // Rotation of a column pair from alpha = |w_p|^2 (v0), beta = |w_q|^2 (v1) and
@@ -734,7 +741,7 @@ __device__ __forceinline__ void svd_body(const MpsView<T>& mps, const SvdWork<T>
             ++sweep;
             break;
         }
-        mixed = still_mixed(mixed, done, N);
+        mixed = still_mixed(mixed, done, N, sweep);
     }
     // column norms -> sig2 (FP64)
     {
@@ -868,7 +875,7 @@ __device__ void jacobi_core(cplx_t<T>* col, const int rc, const int R, const int
             ++sweep;
             break;
         }
-        mixed = still_mixed(mixed, done, N);
+        mixed = still_mixed(mixed, done, N, sweep);
     }
     sweeps = sweep;
     __syncthreads();
@@ -1523,7 +1530,7 @@ __device__ void svd_bgj_body(const MpsView<T>& mps, const SvdWork<T>& wk, const 
             ++sweep;
             break;
         }
-        mixed = still_mixed(mixed, done, N);
+        mixed = still_mixed(mixed, done, N, sweep);
     }
     // column norms -> sig2 (FP64)
     for (int j = warp; j < N; j += NW) {
@@ -1927,7 +1934,7 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
             ++sweep;
             break;
         }
-        mixed = still_mixed(mixed, done, N);
+        mixed = still_mixed(mixed, done, N, sweep);
     }
     if (fail) {
         // every thread leaves together; wait (bounded) for copies still in flight

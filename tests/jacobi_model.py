@@ -10,9 +10,11 @@ sweep and visited in row-cyclic order, as the batched kernel does (it groups the
 8, which changes the order of the pairs but not the rules).
 
 freeze rules:
-  "A": skip a pair when either column is under the floor (the kernels);
+  "A": skip a pair when either column is under the floor;
   "C": skip only pairs with both columns under the floor;
-  "F": C while a sweep still rotates at least 10% of its pairs, then A.
+  "F" (the kernels): while a sweep still rotates at least 10% of its pairs, and for at most
+       4 + 2 log2(N) sweeps, rotate a pair when one column is above the floor and the other
+       holds more than 1e-6 of it; then A.
 """
 from __future__ import annotations
 
@@ -52,7 +54,10 @@ def one_sided_jacobi(A: np.ndarray, rule: str = "A", tol: float = 1e-13, max_swe
                 if late or rule == "A":
                     if not (v0 > tiny and v1 > tiny):
                         continue
-                elif not (v0 > tiny or v1 > tiny):
+                elif rule == "C":
+                    if not (v0 > tiny or v1 > tiny):
+                        continue
+                elif not (max(v0, v1) > tiny and min(v0, v1) > 1e-6 * tiny):
                     continue
                 if not (v2 * v2 + v3 * v3 > tol * tol * v0 * v1):
                     continue
@@ -62,9 +67,10 @@ def one_sided_jacobi(A: np.ndarray, rule: str = "A", tol: float = 1e-13, max_swe
                 W[:, i] = xn
                 W[:, j] = yn
                 rot += 1
-        if rule == "F" and not late and rot < 0.1 * N * (N - 1) / 2:
+        if rule == "F" and not late and (rot < 0.1 * N * (N - 1) / 2 or sweep + 1 >= 4 + 2 * int(np.ceil(np.log2(N)))):
             late = True
-            continue
+            if rot:
+                continue
         if rot == 0:
             sweeps = sweep + 1
             break
