@@ -120,11 +120,13 @@ def job_status(status: int, world: int, device: str = "cuda") -> int:
     return int(max_over_ranks(float(status), world, device=device))
 
 
-def fp64_peak_tflops() -> float:
-    """FP64 peak of this GPU as cuBLAS reaches it: best of 5 DGEMMs of 4096^3 (CUDA events)."""
+def fp64_peak_tflops(dtype=None) -> float:
+    """FP64 (or, with dtype=float32, FP32 CUDA-core) peak of this GPU as cuBLAS reaches it: best of
+    5 GEMMs of 4096^3 (CUDA events; TF32 is off for float32 matmuls by default)."""
     import torch
-    a = torch.randn(4096, 4096, dtype=torch.float64, device="cuda")
-    b = torch.randn(4096, 4096, dtype=torch.float64, device="cuda")
+    dtype = dtype or torch.float64
+    a = torch.randn(4096, 4096, dtype=dtype, device="cuda")
+    b = torch.randn(4096, 4096, dtype=dtype, device="cuda")
     torch.matmul(a, b)
     best = None
     for _ in range(5):
@@ -500,8 +502,12 @@ def main():
         kname = "k_svd (cooperative column-pair Jacobi, 512x512 theta)"
     elif args.jacobi_block == 32:
         kname = "k_svd_bgj_batch (block-Gram Jacobi, one CTA per 512x512 theta)"
+    elif args.jacobi_block == 0:
+        kname = ("k_svd_batch_split (column-pair Jacobi in blocks of 8, each column's rows over two warps, "
+                 "one CTA per 512x512 theta)")
     else:
-        kname = "k_svd_batch (column-pair Jacobi in blocks of 8, one CTA per 512x512 theta)"
+        kname = (f"k_svd_batch (column-pair Jacobi in blocks of {max(4, args.jacobi_block)}, one CTA per "
+                 "512x512 theta)")
     roofline = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak,
                 "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
@@ -509,16 +515,18 @@ def main():
                 "algorithmic_bytes_per_launch": svd_bytes / max(svd_n, 1), "avg_sweeps": sweeps,
                 "svd_share_of_step": svd_ms / ms if ms else None}
 
-    # the Jacobi arithmetic against the FP64 peak (the kernels compute in FP64: c128 data, FP64
-    # dot products and rotations)
+    # the Jacobi arithmetic against the peak of the pipe it runs on: complex128 computes its dot
+    # products and rotations in FP64; complex64 in FP32 (FP64 only for the per-pair cross-lane sums,
+    # the convergence test and the rotation angle)
+    c64 = args.precision == "c64"
     try:
-        p64 = fp64_peak_tflops()
+        p64 = fp64_peak_tflops(torch.float32 if c64 else None)
     except Exception:
         p64 = None
     ach64 = svd_flops / (svd_ms / 1e3) / 1e12 if svd_ms else 0.0
-    compute_roofline = {"kernel": kname, "bound": "fp64", "achieved": ach64, "peak": p64, "unit": "TFLOP/s",
-                        "frac": ach64 / p64 if p64 else None,
-                        "peak_kind": "cuBLAS DGEMM 4096^3 measured in this run (best of 5)",
+    compute_roofline = {"kernel": kname, "bound": "fp32" if c64 else "fp64", "achieved": ach64, "peak": p64,
+                        "unit": "TFLOP/s", "frac": ach64 / p64 if p64 else None,
+                        "peak_kind": f"cuBLAS {'SGEMM' if c64 else 'DGEMM'} 4096^3 measured in this run (best of 5)",
                         "flops_per_launch": svd_flops / max(svd_n, 1)}
 
     # ---- e2e: host-buffer ABI call per step (values from pinned host memory, stats back) ----
