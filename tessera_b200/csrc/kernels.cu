@@ -1638,17 +1638,13 @@ __device__ void bitonic_desc(double* key, int* idx, int P2) {
         }
 }
 
-template <typename T, int BW, int RPL, int S = 1>
+template <typename T, int BW, int RPL>
 __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const SvdParams& pp, unsigned char* smraw) {
     using V = cplx_t<T>;
-    // S = 2: each column's rows are split over two warps (warp w and w + BW hold the first and
-    // second half), twice the resident warps with half the registers each; a pair's partial
-    // dot products are combined through shared memory between the two warps
-    constexpr int NT = 32 * BW * S;
-    constexpr int NW = BW * S;
-    constexpr int RH = RPL / S;       // register rows per lane
+    constexpr int NT = 32 * BW;
+    constexpr int NW = BW;
     constexpr int G2 = 2 * NT / BW;  // threads per pair of the inner rounds (BW/2 pairs)
-    static_assert(RPL > 0 && (S == 1 || S == 2) && RPL % S == 0, "register-resident rows");
+    static_assert(RPL > 0, "register-resident rows");
     __shared__ double red[4 * NW];
     __shared__ int s_rot;
     __shared__ int s_ok;
@@ -1662,11 +1658,9 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
     // cross rounds: column q of the J buffer has been through s_ver[q] rounds since the SVD
     // began; warp w takes column (w + t) % BW in round t once its neighbour w + 1 has released
     // it from round t - 1, so warps are not held in step by a CTA barrier per round
-    __shared__ int s_ver[S][BW];
-    __shared__ double s_part[2][S * BW][4];  // S = 2: per round parity, each warp's partial sums
+    __shared__ int s_ver[BW];
     __shared__ int s_fail;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int cw = warp % BW, hh = warp / BW;  // the warp's column of block I and its half of the rows
     const int R = pp.R > 0 ? pp.R : 2 * mps.dims[pp.bond];
     const int N = pp.N > 0 ? pp.N : 2 * mps.dims[pp.bond + 2];
     const int rc = pp.rows_cap;
@@ -1714,7 +1708,7 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
         return;
     }
     for (int e = tid; e < N; e += NT) { cprev[e] = 1; ccur[e] = 1; }
-    if (tid < S * BW) s_ver[tid / BW][tid % BW] = 0;
+    if (tid < BW) s_ver[tid] = 0;
     if (tid == 0) s_fail = 0;
     int vbase = 0;  // rounds each J column has been through before the current J block
     double rots_total = 0.0;
@@ -1791,12 +1785,12 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
                     __syncthreads();
                 }
             }
-            const bool vi = I * BW + cw < N;
-            V xi[RH];
+            const bool vi = I * BW + warp < N;
+            V xi[RPL];
 #pragma unroll
-            for (int k = 0; k < RH; ++k) {
-                const int row = lane + 32 * (hh * RH + k);
-                xi[k] = row < R ? ci[cw * rc + row] : czero<V>();
+            for (int k = 0; k < RPL; ++k) {
+                const int row = lane + 32 * k;
+                xi[k] = row < R ? ci[warp * rc + row] : czero<V>();
             }
             __syncthreads();  // ci free for the next block I
             if (jn < nb && tid == 0) rc_stage<T>(cj[0], W, ld, rc, R, N, jn, BW, &bars[1], perm);
@@ -1810,12 +1804,12 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
                 moved += 1.0;
                 V* cb = cj[b];
                 for (int t = 0; t < BW; ++t) {
-                    const int q = (cw + t) % BW;
+                    const int q = (warp + t) % BW;
                     const bool ok = vi && (J * BW + q < N);
                     V* cq = cb + q * rc;
                     if (t > 0) {  // bounded wait for warp w + 1 to release column q from round t - 1
                         if (lane == 0) {
-                            const volatile int* vq = &s_ver[hh][q];
+                            const volatile int* vq = &s_ver[q];
                             unsigned spin = 0;
                             while (*vq < vbase + t && !*(volatile int*)&s_fail)
                                 if (++spin > (1u << 24)) { s_fail = 1; break; }
@@ -1823,21 +1817,21 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
                         __syncwarp();
                         __threadfence_block();
                     }
-                    V yj[RH];
+                    V yj[RPL];
 #pragma unroll
-                    for (int k = 0; k < RH; ++k) {
-                        const int row = lane + 32 * (hh * RH + k);
+                    for (int k = 0; k < RPL; ++k) {
+                        const int row = lane + 32 * k;
                         yj[k] = (ok && row < R) ? cq[row] : czero<V>();
                     }
                     double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
                     if constexpr (sizeof(T) == 4) {
                         LaneDotsF32 d;
 #pragma unroll
-                        for (int k = 0; k < RH; ++k) d.add(xi[k], yj[k]);
+                        for (int k = 0; k < RPL; ++k) d.add(xi[k], yj[k]);
                         v0 = d.a; v1 = d.b; v2 = d.gr; v3 = d.gi;
                     } else {
 #pragma unroll
-                        for (int k = 0; k < RH; ++k) {
+                        for (int k = 0; k < RPL; ++k) {
                             const V x = xi[k], y = yj[k];
                             v0 += (double)x.x * x.x + (double)x.y * x.y;
                             v1 += (double)y.x * y.x + (double)y.y * y.y;
@@ -1852,23 +1846,10 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
                         v2 += __shfl_xor_sync(0xffffffffu, v2, o);
                         v3 += __shfl_xor_sync(0xffffffffu, v3, o);
                     }
-                    if constexpr (S == 2) {  // both halves' sums, added in the same order by both warps
-                        if (lane == 0) {
-                            double* mine = s_part[t & 1][warp];
-                            mine[0] = v0; mine[1] = v1; mine[2] = v2; mine[3] = v3;
-                        }
-                        asm volatile("bar.sync %0, %1;" ::"r"(1 + cw), "r"(64) : "memory");
-                        const double* p0 = s_part[t & 1][cw];
-                        const double* p1 = s_part[t & 1][cw + BW];
-                        v0 = p0[0] + p1[0];
-                        v1 = p0[1] + p1[1];
-                        v2 = p0[2] + p1[2];
-                        v3 = p0[3] + p1[3];
-                    }
                     T c, sn, er, ei;
                     if (ok && jacobi_rotation<T>(v0, v1, v2, v3, pp.tol, tiny, mixed, c, sn, er, ei)) {
 #pragma unroll
-                        for (int k = 0; k < RH; ++k) {
+                        for (int k = 0; k < RPL; ++k) {
                             const V x = xi[k], y = yj[k];
                             const T ey_re = er * y.x + ei * y.y, ey_im = er * y.y - ei * y.x;
                             const T ex_re = er * x.x - ei * x.y, ex_im = er * x.y + ei * x.x;
@@ -1876,20 +1857,16 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
                             yj[k] = mk<V>(sn * ex_re + c * y.x, sn * ex_im + c * y.y);
                         }
 #pragma unroll
-                        for (int k = 0; k < RH; ++k) {
-                            const int row = lane + 32 * (hh * RH + k);
+                        for (int k = 0; k < RPL; ++k) {
+                            const int row = lane + 32 * k;
                             if (row < R) cq[row] = yj[k];
                         }
-                        if (lane == 0) {
-                            if (hh == 0) ++rot;
-                            s_jrot = 1;
-                            s_irot = 1;
-                        }
+                        if (lane == 0) { ++rot; s_jrot = 1; s_irot = 1; }
                     }
                     // release column q to warp w - 1 for round t + 1
                     __syncwarp();
                     __threadfence_block();
-                    if (lane == 0) *(volatile int*)&s_ver[hh][q] = vbase + t + 1;
+                    if (lane == 0) *(volatile int*)&s_ver[q] = vbase + t + 1;
                 }
                 vbase += BW;
                 __syncthreads();
@@ -1910,13 +1887,13 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
             }
             if (fail) break;
             const bool i_changed = s_irot != 0;
-            if (i_changed && vi && lane == 0) ccur[perm[I * BW + cw]] = 1;
+            if (i_changed && vi && lane == 0) ccur[perm[I * BW + warp]] = 1;
             if (i_changed) moved += 1.0;
             if (vi && i_changed) {
-                V* dst = W + (long long)perm[I * BW + cw] * ld;
+                V* dst = W + (long long)perm[I * BW + warp] * ld;
 #pragma unroll
-                for (int k = 0; k < RH; ++k) {
-                    const int row = lane + 32 * (hh * RH + k);
+                for (int k = 0; k < RPL; ++k) {
+                    const int row = lane + 32 * k;
                     if (row < R) dst[row] = xi[k];
                 }
             }
@@ -1971,21 +1948,6 @@ __global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd_batch(const In
         pp.bond = rf.op.bond;
         if constexpr (RPL > 0) svd_body_rc<T, BW, RPL>(it.mps, it.wk, pp, smraw);
         else svd_body<T, BW, RPL>(it.mps, it.wk, pp, 0, 1, smraw);
-        __syncthreads();
-    }
-}
-
-// Batched, S = 2: each theta's columns split over two warps each (64 BW threads per CTA).
-template <typename T, int BW, int RPL>
-__global__ void __launch_bounds__(64 * BW, 1) k_svd_batch_split(const InstTask<T>* insts, const UpdRef* refs,
-                                                               int nref) {
-    extern __shared__ __align__(16) unsigned char smraw[];
-    for (int t = blockIdx.x; t < nref; t += gridDim.x) {
-        const UpdRef rf = refs[t];
-        const InstTask<T>& it = insts[rf.inst];
-        SvdParams pp = it.pp;
-        pp.bond = rf.op.bond;
-        svd_body_rc<T, BW, RPL, 2>(it.mps, it.wk, pp, smraw);
         __syncthreads();
     }
 }
@@ -2559,23 +2521,6 @@ static void svd_batch_bw(const InstTask<T>* insts, const UpdRef* refs, int nref,
     TQ_CHECK(cudaGetLastError());
 }
 
-template <typename T, int BW, int RPL>
-static void svd_batch_split(const InstTask<T>* insts, const UpdRef* refs, int nref, int rows_cap, cudaStream_t s) {
-    using V = cplx_t<T>;
-    size_t smem = sizeof(V) * 3 * BW * (size_t)rows_cap;
-    const size_t sort_smem = 4096 * (sizeof(double) + sizeof(int));
-    if (smem < sort_smem) smem = sort_smem;
-    auto fn = k_svd_batch_split<T, BW, RPL>;
-    TQ_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    TQ_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 64 * BW, smem));
-    if (per_sm < 1) throw std::runtime_error("k_svd_batch_split does not fit on an SM");
-    int grid = per_sm * num_sms();
-    if (grid > nref) grid = nref;
-    fn<<<grid, 64 * BW, smem, s>>>(insts, refs, nref);
-    TQ_CHECK(cudaGetLastError());
-}
-
 // complex64 at 512 rows: blocks of 16 columns (512 threads, 16 warps); a complex128 column pair
 // of 512 rows does not fit in the registers that 16 warps leave each thread
 template <typename T>
@@ -2620,9 +2565,6 @@ void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref,
     } else if (block_w == BG_B) {
         bgj_launch<T>(nullptr, nullptr, nullptr, insts, refs, nref, s);
     } else if (bw == 16 && rpl == 16 && svd_batch_wide<T>(insts, refs, nref, rows_cap, s)) {
-    } else if (block_w == 0 && rpl == 16) {
-        // 257..512 rows by default: blocks of 8 columns, each column's rows over two warps
-        svd_batch_split<T, 8, 16>(insts, refs, nref, rows_cap, s);
     } else {
 #define TQ_RB(B, RP) \
     if (bw == B && rpl == RP) { svd_batch_bw<T, B, RP>(insts, refs, nref, rows_cap, s); } else
