@@ -502,12 +502,9 @@ def main():
         kname = "k_svd (cooperative column-pair Jacobi, 512x512 theta)"
     elif args.jacobi_block == 32:
         kname = "k_svd_bgj_batch (block-Gram Jacobi, one CTA per 512x512 theta)"
-    elif args.jacobi_block == 0:
-        kname = ("k_svd_batch_split (column-pair Jacobi in blocks of 8, each column's rows over two warps, "
-                 "one CTA per 512x512 theta)")
     else:
-        kname = (f"k_svd_batch (column-pair Jacobi in blocks of {max(4, args.jacobi_block)}, one CTA per "
-                 "512x512 theta)")
+        bw = args.jacobi_block or (16 if args.precision == "c64" else 8)
+        kname = f"k_svd_batch (column-pair Jacobi in blocks of {max(4, bw)}, one CTA per 512x512 theta)"
     roofline = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak,
                 "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,

@@ -298,15 +298,15 @@ __device__ __forceinline__ bool pair_live(const double v0, const double v1, cons
 }
 
 // Whether the next sweep stays in the mixed phase: this sweep rotated at least 10% of the pairs,
-// and the phase has not yet lasted 4 + 2 log2(N) sweeps.  The cap bounds the phase on the rare
+// and the phase has not yet lasted 8 + 3 log2(N) sweeps.  The cap bounds the phase on the rare
 // theta where a few mixed pairs keep rotating by rounding (seen on small exact-chi theta: the
 // count then stays above 10% of a handful of pairs and the sweeps never settle); the late rule
-// converges from there.  Random 1024-column matrices leave the phase after 17 sweeps, under
-// the cap of 24.
+// converges from there.  It leaves room for the slower tournament order of the cooperative
+// kernel on 1024 columns (cap 38).
 __device__ __forceinline__ bool still_mixed(const bool mixed, const double rotated, const int N, const int sweep) {
     int lg = 0;
     while ((1 << lg) < N) ++lg;
-    return mixed && rotated >= 0.05 * (double)N * (double)(N - 1) && sweep + 1 < 4 + 2 * lg;
+    return mixed && rotated >= 0.05 * (double)N * (double)(N - 1) && sweep + 1 < 8 + 3 * lg;
 }
 
 // Rotation of a column pair from alpha = |w_p|^2 (v0), beta = |w_q|^2 (v1) and
@@ -2559,8 +2559,9 @@ void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref,
     rp.rows_cap = rows_cap;
     rp.cols_cap = rows_cap;  // every instance's theta is at most rows_ub x rows_ub
     // small theta: resident Jacobi; large theta: the column-pair kernel (block width 8, or the
-    // one asked for), or the block-Gram kernel when block width 32 is asked for
-    if (block_w == 0) bw = 8;
+    // one asked for; complex64 at 257..512 rows: 16), or the block-Gram kernel when block width
+    // 32 is asked for
+    if (block_w == 0) bw = (sizeof(T) == 4 && rpl == 16) ? 16 : 8;
     if (res_dispatch<T>(nullptr, nullptr, rp, insts, refs, nref, s)) {
     } else if (block_w == BG_B) {
         bgj_launch<T>(nullptr, nullptr, nullptr, insts, refs, nref, s);

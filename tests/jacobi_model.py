@@ -13,7 +13,7 @@ freeze rules:
   "A": skip a pair when either column is under the floor;
   "C": skip only pairs with both columns under the floor;
   "F" (the kernels): while a sweep still rotates at least 10% of its pairs, and for at most
-       4 + 2 log2(N) sweeps, rotate a pair when one column is above the floor and the other
+       8 + 3 log2(N) sweeps, rotate a pair when one column is above the floor and the other
        holds more than 1e-6 of it; then A.
 """
 from __future__ import annotations
@@ -67,7 +67,7 @@ def one_sided_jacobi(A: np.ndarray, rule: str = "A", tol: float = 1e-13, max_swe
                 W[:, i] = xn
                 W[:, j] = yn
                 rot += 1
-        if rule == "F" and not late and (rot < 0.1 * N * (N - 1) / 2 or sweep + 1 >= 4 + 2 * int(np.ceil(np.log2(N)))):
+        if rule == "F" and not late and (rot < 0.1 * N * (N - 1) / 2 or sweep + 1 >= 8 + 3 * int(np.ceil(np.log2(N)))):
             late = True
             if rot:
                 continue
