@@ -365,6 +365,22 @@ struct LaneDotsF32 {
     }
 };
 
+// The rotation w_p <- c w_p - s conj(e) w_q, w_q <- s e w_p + c w_q as x' = c x + b y,
+// y' = d x + c y with the complex coefficients b = -s conj(e) and d = s e formed once per pair:
+// 12 real multiply-adds per row instead of 16.
+template <typename T>
+struct PairRot {
+    T c, br, bi, dr, di;
+    __device__ __forceinline__ PairRot(T c_, T s, T er, T ei) : c(c_), br(-s * er), bi(s * ei), dr(s * er), di(s * ei) {}
+    __device__ __forceinline__ void apply(cplx_t<T>& x, cplx_t<T>& y) const {
+        const cplx_t<T> xo = x, yo = y;
+        x.x = fma(-bi, yo.y, fma(br, yo.x, c * xo.x));
+        x.y = fma(bi, yo.x, fma(br, yo.y, c * xo.y));
+        y.x = fma(-di, xo.y, fma(dr, xo.x, c * yo.x));
+        y.y = fma(di, xo.x, fma(dr, xo.y, c * yo.y));
+    }
+};
+
 // Rotate local columns p, q (shared memory) of a group; returns 1 if rotated.
 template <typename T, int G>
 __device__ __forceinline__ int rotate_pair(cplx_t<T>* cp, cplx_t<T>* cq, bool valid, int R, double tol,
@@ -391,13 +407,12 @@ __device__ __forceinline__ int rotate_pair(cplx_t<T>* cp, cplx_t<T>* cq, bool va
     if (!valid) return 0;
     T cc, ss, er, ei;
     if (!jacobi_rotation<T>(v[0], v[1], v[2], v[3], tol, tiny, mixed, cc, ss, er, ei)) return 0;
+    const PairRot<T> rt(cc, ss, er, ei);
     for (int r = lg; r < R; r += G) {
-        const V x = cp[r], y = cq[r];
-        // s conj(e) y and s e x
-        const T ey_re = er * y.x + ei * y.y, ey_im = er * y.y - ei * y.x;
-        const T ex_re = er * x.x - ei * x.y, ex_im = er * x.y + ei * x.x;
-        cp[r] = mk<V>(cc * x.x - ss * ey_re, cc * x.y - ss * ey_im);
-        cq[r] = mk<V>(ss * ex_re + cc * y.x, ss * ex_im + cc * y.y);
+        V x = cp[r], y = cq[r];
+        rt.apply(x, y);
+        cp[r] = x;
+        cq[r] = y;
     }
     return 1;
 }
@@ -697,14 +712,9 @@ __device__ __forceinline__ void svd_body(const MpsView<T>& mps, const SvdWork<T>
                         }
                         T c, sn, er, ei;
                         if (ok && jacobi_rotation<T>(v0, v1, v2, v3, pp.tol, tiny, mixed, c, sn, er, ei)) {
+                            const PairRot<T> rt(c, sn, er, ei);
 #pragma unroll
-                            for (int k = 0; k < RPL; ++k) {
-                                const V x = xi[k], y = yj[k];
-                                const T ey_re = er * y.x + ei * y.y, ey_im = er * y.y - ei * y.x;
-                                const T ex_re = er * x.x - ei * x.y, ex_im = er * x.y + ei * x.x;
-                                xi[k] = mk<V>(c * x.x - sn * ey_re, c * x.y - sn * ey_im);
-                                yj[k] = mk<V>(sn * ex_re + c * y.x, sn * ex_im + c * y.y);
-                            }
+                            for (int k = 0; k < RPL; ++k) rt.apply(xi[k], yj[k]);
 #pragma unroll
                             for (int k = 0; k < RPL; ++k) {
                                 const int row = lane + 32 * k;
@@ -846,16 +856,16 @@ __device__ void jacobi_core(cplx_t<T>* col, const int rc, const int R, const int
                 }
                 T c, sn, er, ei;
                 if (ok && jacobi_rotation<T>(v0, v1, v2, v3, tol, tiny, mixed, c, sn, er, ei)) {
+                    const PairRot<T> rt(c, sn, er, ei);
 #pragma unroll
                     for (int k = 0; k < RPL; ++k) {
                         if (k >= rpl) break;
                         const int row = sl + LPP * k;
-                        const V xv = x[k], yv = y[k];
-                        const T ey_re = er * yv.x + ei * yv.y, ey_im = er * yv.y - ei * yv.x;
-                        const T ex_re = er * xv.x - ei * xv.y, ex_im = er * xv.y + ei * xv.x;
+                        V xv = x[k], yv = y[k];
+                        rt.apply(xv, yv);
                         if (row < R) {
-                            cp[row] = mk<V>(c * xv.x - sn * ey_re, c * xv.y - sn * ey_im);
-                            cq[row] = mk<V>(sn * ex_re + c * yv.x, sn * ex_im + c * yv.y);
+                            cp[row] = xv;
+                            cq[row] = yv;
                         }
                     }
                     if (sl == 0) ++rot;
@@ -1848,14 +1858,9 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
                     }
                     T c, sn, er, ei;
                     if (ok && jacobi_rotation<T>(v0, v1, v2, v3, pp.tol, tiny, mixed, c, sn, er, ei)) {
+                        const PairRot<T> rt(c, sn, er, ei);
 #pragma unroll
-                        for (int k = 0; k < RPL; ++k) {
-                            const V x = xi[k], y = yj[k];
-                            const T ey_re = er * y.x + ei * y.y, ey_im = er * y.y - ei * y.x;
-                            const T ex_re = er * x.x - ei * x.y, ex_im = er * x.y + ei * x.x;
-                            xi[k] = mk<V>(c * x.x - sn * ey_re, c * x.y - sn * ey_im);
-                            yj[k] = mk<V>(sn * ex_re + c * y.x, sn * ex_im + c * y.y);
-                        }
+                        for (int k = 0; k < RPL; ++k) rt.apply(xi[k], yj[k]);
 #pragma unroll
                         for (int k = 0; k < RPL; ++k) {
                             const int row = lane + 32 * k;
