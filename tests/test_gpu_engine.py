@@ -66,8 +66,8 @@ def test_svd_kernel_matches_reference_spectra(golden):
 @pytest.mark.parametrize("shape", [(64, 64), (128, 96), (512, 512), (200, 300), (2048, 256), (1024, 1024)])
 def test_svd_kernel_large_random(shape):
     """Random unitary factors around a TEBD-like spectrum exp(-k/20).  Values above the
-    kernel's noise floor (8 sqrt(R) ulps of ||A||_F) are resolved to 1e-9 relative; those under
-    it come back under twice it.  At 1024 x 1024, 437 of the values lie under the floor, and
+    kernel's noise floor (8 sqrt(R) ulps of ||A||_F) are resolved to 1e-9 relative or 1% of the
+    floor absolute; those under it come back under twice it.  At 1024 x 1024, 437 of the values lie under the floor, and
     columns whose norm dips under it mid-sweep must still be orthogonalised against the resolved
     ones (the early, mixed phase of the freeze rule), else values a few times the floor come
     back at it and U loses orthogonality."""
@@ -79,8 +79,8 @@ def test_svd_kernel_large_random(shape):
     u, sg, vh = ffi.svd(A)
     floor = 8.0 * np.sqrt(max(shape)) * np.finfo(np.float64).eps * np.linalg.norm(A)
     assert np.allclose(sg, s, rtol=1e-9, atol=floor)
-    above = s > 4 * floor
-    assert np.max(np.abs(sg[above] - s[above]) / s[above]) < 1e-4
+    above = s > 4 * floor  # resolved: off by a small fraction of the floor (a frozen column is off by ~ the floor)
+    assert np.max(np.abs(sg[above] - s[above])) < 0.01 * floor
     assert np.max(sg[s < floor]) <= 2 * floor if np.any(s < floor) else True
     assert np.linalg.norm(u.conj().T @ u - np.eye(len(s))) < 1e-9
     assert np.linalg.norm(u @ np.diag(sg) @ vh - A) < 1e-11 * np.linalg.norm(A)
