@@ -299,23 +299,34 @@ def config_dict(args, p):
 # ------------------------------------------------------------------------------------
 # tessera engine
 # ------------------------------------------------------------------------------------
-def plain_rate(args, local):
-    """Plain single-instance engine (cooperative SVD over all SMs) on one instance, same gates."""
-    import torch
-
+def plain_rate(args, local, peak_gbs=None, peak_tflops=None):
+    """Plain single-instance engine (cooperative SVD over all SMs) on one instance, same gates;
+    returns (updates/s, ms per update, roofline of its SVD kernel or None)."""
     from tessera_b200 import ffi
     p = workload(args, 0)
     s = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=args.chi, precision=args.precision,
-                    kernel_timing=False, device=local)
+                    kernel_timing=True, device=local)
     s.randomize(1234)
     lo = 16 * min(32, args.n // 4)
     s.run_gates(MID_STEP, lo, lo + 2)
-    s.sync()
+    r0 = s.sync()
     g = max(2, args.gates // 2)
     s.run_gates(MID_STEP, lo + 2, lo + 2 + g)
     r = s.sync()
     s.close()
-    return g / (r.device_ms / 1e3), r.device_ms / g
+    n = r.svd_launches - r0.svd_launches
+    ms = r.svd_ms - r0.svd_ms
+    roof = None
+    if n and ms > 0:
+        gbs = (r.svd_bytes - r0.svd_bytes) / (ms / 1e3) / 1e9
+        tfl = (r.svd_flops - r0.svd_flops) / (ms / 1e3) / 1e12
+        roof = {"kernel": "k_svd (cooperative column-pair Jacobi, 512x512 theta)", "avg_launch_ms": ms / n,
+                "sweeps_per_update": (r.svd_sweeps - r0.svd_sweeps) / max(r.two_site_updates - r0.two_site_updates, 1),
+                "hbm": {"achieved": gbs, "unit": "GB/s", "peak": peak_gbs,
+                        "frac": gbs / peak_gbs if peak_gbs else None},
+                "compute": {"achieved": tfl, "unit": "TFLOP/s", "peak": peak_tflops,
+                            "frac": tfl / peak_tflops if peak_tflops else None}}
+    return g / (r.device_ms / 1e3), r.device_ms / g, roof
 
 
 def solves(args):
@@ -566,9 +577,9 @@ def main():
     if B > 1 and rank == 0:
         sess.close()
         try:
-            pr, pms = plain_rate(args, local)
+            pr, pms, proof = plain_rate(args, local, peak, p64)
             plain = {"value": pr, "unit": UNIT, "ms_per_update": pms,
-                     "engine": "plain single-instance, cooperative SVD across all SMs"}
+                     "engine": "plain single-instance, cooperative SVD across all SMs", "roofline": proof}
         except Exception as exc:
             plain = {"value": None, "error": str(exc)}
 
