@@ -907,6 +907,10 @@ public:
     ~BatchEngine() override { release(); }
     void release() noexcept {
         if (st_) cudaStreamSynchronize(st_);
+        if (gexec_) cudaGraphExecDestroy(gexec_);
+        if (graph_) cudaGraphDestroy(graph_);
+        gexec_ = nullptr;
+        graph_ = nullptr;
         for (cudaEvent_t e : pool_) cudaEventDestroy(e);
         if (e0_) cudaEventDestroy(e0_);
         if (e1_) cudaEventDestroy(e1_);
@@ -1084,13 +1088,35 @@ public:
             sync(nullptr);
             return;
         }
+        // One Trotter step is the same launch sequence for every k (the kernels read the step
+        // from the device counter), so without per-launch timing it is captured once into a CUDA
+        // graph and replayed: one launch per step instead of 4 per gate slot.
+        const bool graph = !timing_ && k1 - k0 >= 2;
+        if (graph && !gexec_) {
+            cudaGraph_t g = nullptr;
+            const long long l0 = launches_, s0 = svd_launches_;  // capturing launches nothing
+            TQ_CK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+            try {
+                step_body(B);
+            } catch (...) {
+                cudaStreamEndCapture(st_, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            TQ_CK(cudaStreamEndCapture(st_, &g));
+            launches_ = l0;
+            svd_launches_ = s0;
+            graph_ = g;
+            TQ_CK(cudaGraphInstantiate(&gexec_, graph_, 0));
+        }
         for (int k = k0; k < k1; ++k) {
-            launch_single_site_batch<T>(insts_, B, n_max_, cap_max_ * cap_max_, st_);
-            for (int q = 0; q < q_max_; ++q) slot(q);
-            launch_single_site_batch<T>(insts_, B, n_max_, cap_max_ * cap_max_, st_);
-            launch_entropy_batch<T>(insts_, B, st_);
-            launch_step_inc(step_, st_);
-            launches_ += 4;
+            if (graph) {
+                TQ_CK(cudaGraphLaunch(gexec_, st_));
+                launches_ += 4 + 4LL * q_max_;
+                svd_launches_ += q_max_;
+            } else {
+                step_body(B);
+            }
         }
         TQ_CK(cudaEventRecord(e1_, st_));
         ran_ = true;
@@ -1100,6 +1126,16 @@ public:
     long long launches() const { return launches_; }
 
 private:
+    // one Trotter step of every instance: half single-site gates, every gate slot, half
+    // single-site gates, the qubit-0 entropy, the step counter
+    void step_body(int B) {
+        launch_single_site_batch<T>(insts_, B, n_max_, cap_max_ * cap_max_, st_);
+        for (int q = 0; q < q_max_; ++q) slot(q);
+        launch_single_site_batch<T>(insts_, B, n_max_, cap_max_ * cap_max_, st_);
+        launch_entropy_batch<T>(insts_, B, st_);
+        launch_step_inc(step_, st_);
+        launches_ += 4;
+    }
     // gate slot q of every instance that has one: theta, Jacobi SVD, absorption
     void slot(int q) {
         const int nref = (int)(refs_off_[q + 1] - refs_off_[q]);
@@ -1135,6 +1171,8 @@ private:
     std::vector<std::unique_ptr<Engine<T>>> eng_;
     cudaStream_t st_ = nullptr;
     cudaEvent_t e0_ = nullptr, e1_ = nullptr;
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t gexec_ = nullptr;
     char* base_ = nullptr;
     int* step_ = nullptr;
     InstTask<T>* insts_ = nullptr;

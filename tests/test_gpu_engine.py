@@ -615,3 +615,23 @@ def test_truncating_chi256_updates_match_the_oracle(chi256_window, batched):
     for i, (g, o) in enumerate(zip(g_sites, o_sites)):
         ng, no = left_norms(g), left_norms(o)
         assert np.max(np.abs(ng - no) / no) < 1e-10, i
+
+
+def test_graph_captured_steps_equal_launched_steps():
+    """The batched slot path captures one Trotter step into a CUDA graph and replays it for every
+    step when no per-launch timing is asked for; with kernel timing it launches kernel by
+    kernel. Same batch (128-row theta: too big for the resident kernel), same steps: the states,
+    the discarded weight and the launch counts are identical."""
+    probs = [instances.chain_range(n=12, dmax=3, seed=s, T=1.0, dt=0.05, chi=64) for s in (1, 2)]
+    out = []
+    for timing in (False, True):
+        sb = ffi.Session.batch(probs, chi=64, kernel_timing=timing)
+        sb.run(0, 6)
+        r = sb.sync()
+        assert r.status == 0
+        out.append(([sb.save_instance(b) for b in range(len(probs))], r.max_trunc, r.two_site_updates,
+                    r.svd_launches))
+        sb.close()
+    assert out[0][0] == out[1][0]
+    assert out[0][1:] == out[1][1:]
+    assert out[0][3] == 6 * max(p.updates_per_step() for p in probs)
