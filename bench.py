@@ -51,8 +51,8 @@ def parse():
     ap.add_argument("--batch", type=int, default=148, help="instances per GPU (1 = plain single-instance engine)")
     ap.add_argument("--gates", type=int, default=8, help="gate slots per bench step")
     ap.add_argument("--impl", choices=["tessera", "reference"], default="tessera")
-    ap.add_argument("--ref-chi", type=int, default=128,
-                    help="bond dimension the reference arm times (extrapolated to --chi when smaller)")
+    ap.add_argument("--ref-chi", type=int, default=64,
+                    help="bond dimension the reference arm times (scaled to --chi when smaller)")
     ap.add_argument("--precision", choices=["c128", "c64"], default="c128")
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--dmax", type=int, default=4)
@@ -220,25 +220,40 @@ REF_DIRECT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles"
 
 class RefModel:
     """Reference cost of saturated chi=256 updates on the host cores.  A direct chi=256 update
-    (512 x 512 theta, MPS::apply_adjacent) takes minutes on one core, so by default a step times
-    one chi=128 update (256 x 256 theta) on every host thread at once and extrapolates to
-    chi=256 with the cost exponent between chi=64 and chi=128, both measured at the same
-    concurrency.  --ref-chi 256 times chi=256 updates directly (no extrapolation); the record of
-    such a run (profiles/reference_update_chi256.json) is quoted beside the extrapolated value."""
+    (512 x 512 theta, MPS::apply_adjacent) takes about 17 minutes per thread with 16 threads
+    busy, so it is measured once per pool (--ref-chi 256; profiles/reference_update_chi256.json)
+    together with the same concurrency's chi=64 time.  A default step times one chi=64 update on
+    every host thread at once and scales it to chi=256 by that recorded ratio, i.e. the direct
+    chi=256 rate corrected by how fast this box's cores run the chi=64 update.  Without the
+    record, the cost exponent between chi=64 and chi=128, timed at the same concurrency, is
+    used instead."""
 
-    def __init__(self, chi: int = 128, target: int = 256):
+    def __init__(self, chi: int = 64, target: int = 256):
         self.threads = max(1, min(len(os.sched_getaffinity(0)), 64))
         self.chi, self.target = chi, target
-        self.p = 3.0
+        self.cal = None
+        self.p = None
         self.t_lo = None
-        if chi < target:
+        if chi >= target:
+            return
+        if os.path.exists(REF_DIRECT):
+            with open(REF_DIRECT) as f:
+                rd = json.load(f)
+            c = rd.get("calibration", {})
+            key = f"chi{chi}_seconds"
+            if rd.get("chi") == target and key in c:
+                self.cal = {"t_target": rd["seconds"], "t_chi": c[key], "threads": rd["threads"],
+                            "value": rd["value"]}
+        if self.cal is None:
             self.t_lo, _ = ref_update_sample(chi // 2, self.threads, seed=1)
 
     def step(self, seed=3):
         import math
-        t, per = ref_update_sample(self.chi, self.threads, seed=seed)
+        t, _ = ref_update_sample(self.chi, self.threads, seed=seed)
         if self.chi >= self.target:
             return t, self.threads / t
+        if self.cal is not None:
+            return t, self.threads / (t * self.cal["t_target"] / self.cal["t_chi"])
         self.p = math.log2(t / self.t_lo)
         return t, self.threads / (t * (self.target / self.chi) ** self.p)
 
@@ -246,16 +261,15 @@ class RefModel:
         if self.chi >= self.target:
             return (f"{self.threads} concurrent reference MPS::apply_adjacent updates of a saturated chi={self.chi} "
                     f"bond ({2 * self.chi}x{2 * self.chi} complex128 theta), measured directly: {t:.1f} s")
-        d = (f"{self.threads} concurrent reference MPS::apply_adjacent updates of a saturated chi={self.chi} bond "
-             f"({2 * self.chi}x{2 * self.chi} complex128 theta) took {t:.1f} s; extrapolated to chi={self.target} "
-             f"with the cost exponent {self.p:.2f} measured between chi={self.chi // 2} ({self.t_lo:.2f} s) and "
-             f"chi={self.chi} at the same concurrency")
-        if os.path.exists(REF_DIRECT):
-            with open(REF_DIRECT) as f:
-                rd = json.load(f)
-            d += (f"; a direct chi={rd['chi']} measurement on this pool ({rd['threads']} threads, "
-                  f"{rd['seconds']:.0f} s wall) gave {rd['value']:.4g} updates/s")
-        return d
+        head = (f"{self.threads} concurrent reference MPS::apply_adjacent updates of a saturated chi={self.chi} bond "
+                f"({2 * self.chi}x{2 * self.chi} complex128 theta) took {t:.1f} s; ")
+        if self.cal is not None:
+            c = self.cal
+            return head + (f"scaled to chi={self.target} by the ratio measured directly on this pool with "
+                           f"{c['threads']} threads (chi={self.target}: {c['t_target']:.0f} s, chi={self.chi}: "
+                           f"{c['t_chi']:.2f} s; the direct chi={self.target} rate was {c['value']:.4g} updates/s)")
+        return head + (f"extrapolated to chi={self.target} with the cost exponent {self.p:.2f} measured between "
+                       f"chi={self.chi // 2} ({self.t_lo:.2f} s) and chi={self.chi} at the same concurrency")
 
 
 def run_reference(args):
