@@ -58,6 +58,11 @@ def parse():
     ap.add_argument("--dmax", type=int, default=4)
     ap.add_argument("--chi", type=int, default=256)
     ap.add_argument("--jacobi-block", type=int, default=0)
+    ap.add_argument("--graded-decay", type=float, default=24.0,
+                    help="also time the step on random MPS with graded spectra (site column b scaled by "
+                         "exp(-b/decay)); 0 = skip")
+    ap.add_argument("--precondition", choices=["on", "off"], default="on",
+                    help="pivoted LQ of theta before the batched Jacobi (fewer sweeps)")
     ap.add_argument("--theta-tc", action="store_true",
                     help="complex64: bond contraction on the tcgen05 tensor cores (split-TF32)")
     ap.add_argument("--autotune", action="store_true",
@@ -456,7 +461,8 @@ def main():
                            jacobi_block=args.jacobi_block, kernel_timing=True, device=local)
     else:
         sess = ffi.Session.batch(probs, chi=args.chi, precision=args.precision, jacobi_block=args.jacobi_block,
-                                 kernel_timing=True, device=local, theta_tensor_cores=args.theta_tc)
+                                 kernel_timing=True, device=local, theta_tensor_cores=args.theta_tc,
+                                 jacobi_precondition=1 if args.precondition == "on" else 2)
     sess.randomize(1234 + 1000 * rank)
     G = upd_per_step_inst
     # Gate slots of edges (i, i+d) with 32 <= i < 96: every bond they touch sits at chi = 256
@@ -507,6 +513,7 @@ def main():
     value = updates * world / (ms_max / 1e3)
     svd_n = r1.svd_launches - r0.svd_launches
     svd_ms = r1.svd_ms - r0.svd_ms
+    lq_ms = r1.precond_ms - r0.precond_ms
     svd_bytes = r1.svd_bytes - r0.svd_bytes
     svd_flops = r1.svd_flops - r0.svd_flops
     launches = r1.kernel_launches - r0.kernel_launches
@@ -551,6 +558,22 @@ def main():
                         "peak_kind": f"cuBLAS {'SGEMM' if c64 else 'DGEMM'} 4096^3 measured in this run (best of 5)",
                         "flops_per_launch": svd_flops / max(svd_n, 1)}
 
+    # the pivoted-LQ preconditioner (k_lq_batch): its own launches, timed apart from the Jacobi;
+    # algorithmic bytes per theta: two reads of theta (row norms, first products), then per
+    # elimination step one read and one write of the trailing block
+    precond = None
+    if B > 1 and args.precondition == "on" and lq_ms > 0:
+        R = Nc = 2 * args.chi
+        esz = 16 if args.precision == "c128" else 8
+        lq_bytes = esz * (2 * R * Nc + 2 * sum((R - k) * (Nc - k) for k in range(min(R, Nc))))
+        lq_per_launch = B * lq_bytes
+        lq_avg = lq_ms / max(svd_n, 1)
+        precond = {"kernel": "k_lq_batch (row-pivoted Householder LQ, one CTA per 512x512 theta)",
+                   "avg_launch_ms": lq_avg, "share_of_step": lq_ms / ms if ms else None,
+                   "algorithmic_bytes_per_launch": lq_per_launch,
+                   "achieved": lq_per_launch / (lq_avg / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                   "frac": lq_per_launch / (lq_avg / 1e3) / 1e9 / peak}
+
     # ---- e2e: host-buffer ABI call per step (values from pinned host memory, stats back) ----
     e2e = None
     if not args.no_e2e:
@@ -587,6 +610,39 @@ def main():
                "api": "tessera_qa_session_run_host (h, J, schedule of every instance from pinned host memory -> "
                       f"{G} gate slots -> run statistics to host)"}
 
+    # ---- the same step on states whose spectra fall off like a TEBD state's Schmidt values ----
+    graded = None
+    if args.graded_decay > 0 and B > 1:
+        sess.randomize(1234 + 1000 * rank, decay=args.graded_decay)
+        for w in range(args.warmup):
+            step(w)
+        g0 = sess.sync()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for k in range(args.steps):
+            step(args.warmup + k)
+        e1.record(stream)
+        g1 = sess.sync()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        gms = max_over_ranks(e0.elapsed_time(e1), world)
+        gup = g1.two_site_updates - g0.two_site_updates
+        st = job_status(g1.status, world)
+        if st:
+            raise RuntimeError(f"engine status bits {st} in the graded-spectrum steps (largest over ranks)")
+        gn = g1.svd_launches - g0.svd_launches
+        graded = {"value": gup * world / (gms / 1e3), "unit": UNIT, "decay": args.graded_decay,
+                  "avg_sweeps": (g1.svd_sweeps - g0.svd_sweeps) / max(gup, 1),
+                  "svd_avg_launch_ms": (g1.svd_ms - g0.svd_ms) / max(gn, 1),
+                  "precond_avg_launch_ms": (g1.precond_ms - g0.precond_ms) / max(gn, 1),
+                  "workload": "the headline's instances, gate windows and step count on seeded random MPS whose "
+                              f"site column b is scaled by exp(-b/{args.graded_decay:g}): each theta's singular "
+                              "values fall off like a TEBD state's Schmidt values (the 256th ~1e-7 of the largest "
+                              "before the gate) instead of staying flat"}
+
     plain = None
     if B > 1 and rank == 0:
         sess.close()
@@ -618,7 +674,8 @@ def main():
 
     if rank == 0:
         cfg = config_dict(args, p)
-        cfg.update({"jacobi_block": args.jacobi_block, "theta_tensor_cores": bool(args.theta_tc), "autotune": tuned})
+        cfg.update({"jacobi_block": args.jacobi_block, "theta_tensor_cores": bool(args.theta_tc), "autotune": tuned,
+                    "jacobi_precondition": args.precondition if B > 1 else "off (cooperative single-instance SVD)"})
         cfg.update({"instances_per_gpu": B, "gates_per_step": G,
                     "step": f"{G} consecutive gate slots of the Trotter step at s=0.5 on each of {B} instances"})
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -626,7 +683,9 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "c128" else "f32",
                 "data": "synthetic: seeded Ising instances (PCG64 seeds 2..) and seeded random MPS with every "
                         "bond at its cap",
-                "config": cfg, "roofline": roofline, "compute_roofline": compute_roofline, "cpu_baseline": cpu,
+                "config": cfg, "roofline": roofline, "compute_roofline": compute_roofline, "preconditioner": precond,
+                "graded_spectra": graded,
+                "cpu_baseline": cpu,
                 "e2e": e2e,
                 "gpu_launches": launches, "clocks": ck, "plain_single_instance": plain, "solves": sol,
                 "max_trunc_in_timed_steps": r1.max_trunc}

@@ -96,7 +96,11 @@ typedef struct tessera_qa_config {
     int kernel_timing;      /* 1 = time every Jacobi-SVD launch with CUDA events (result.svd_ms) */
     int theta_tensor_cores; /* complex64 only: 1 = bond contraction on the tcgen05 tensor cores in split-TF32
                                (three TF32 passes, FP32 accumulators); 0 = CUDA-core FP32 */
-    int reserved[5];
+    int jacobi_precondition;/* batched column-pair Jacobi (theta above 256 rows): 0 = default (on), 1 = on,
+                               2 = off.  On: a row-pivoted Householder LQ of theta (P^T theta = L Q^H) runs
+                               first and the Jacobi works on L, which takes fewer sweeps (Drmac-Veselic
+                               preconditioning); the results are the same up to rounding */
+    int reserved[4];
 } tessera_qa_config;
 
 typedef struct tessera_qa_result {
@@ -126,7 +130,8 @@ typedef struct tessera_qa_result {
     long long svd_sweeps;   /* Jacobi sweeps summed over launches */
     long long kernel_launches; /* all engine kernel launches */
     double svd_flops;       /* flops of the Jacobi arithmetic: dot products, rotations, Gram and apply GEMMs */
-    double reserved_d[1];
+    double precond_ms;      /* summed duration of the pivoted-LQ preconditioner launches (config.kernel_timing;
+                               config.jacobi_precondition) */
 } tessera_qa_result;
 
 /* Fills `cfg` with the legacy defaults: dt 0.1, zz_substeps 1, complex128, chi 32. */
@@ -274,6 +279,11 @@ TESSERA_QA_API tessera_qa_session* tessera_qa_session_create_batch(const tessera
 /* Replaces the state by a seeded random MPS with every bond at its cap (min(chi, 2^i,
  * 2^(n-i))), sites scaled so theta stays O(1). */
 TESSERA_QA_API int tessera_qa_session_randomize(tessera_qa_session* s, uint64_t seed);
+/* As tessera_qa_session_randomize, with column b of every site tensor scaled by exp(-b / decay),
+ * so that each two-site theta has a graded singular spectrum (Schmidt values falling off as in a
+ * TEBD state) instead of a flat one; decay 0 is tessera_qa_session_randomize.  A benchmark and
+ * test input, like tessera_qa_session_randomize; the reference has neither. */
+TESSERA_QA_API int tessera_qa_session_randomize_graded(tessera_qa_session* s, uint64_t seed, double decay);
 /* Enqueues Trotter steps [step_begin, step_begin + nsteps) on the session's stream; returns
  * without waiting. */
 TESSERA_QA_API int tessera_qa_session_run(tessera_qa_session* s, size_t step_begin, size_t nsteps);

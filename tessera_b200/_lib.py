@@ -35,7 +35,8 @@ class Config(C.Structure):
                 ("jacobi_tol", C.c_double), ("jacobi_max_sweeps", C.c_int), ("jacobi_block", C.c_int),
                 ("device", C.c_int), ("step_begin", C.c_size_t), ("step_end", C.c_size_t),
                 ("initial_mps", C.c_void_p), ("skip_observables", C.c_int), ("kernel_timing", C.c_int),
-                ("theta_tensor_cores", C.c_int), ("reserved", C.c_int * 5)]
+                ("theta_tensor_cores", C.c_int), ("jacobi_precondition", C.c_int),
+                ("reserved", C.c_int * 4)]
 
 
 class Result(C.Structure):
@@ -46,7 +47,7 @@ class Result(C.Structure):
                 ("max_bond", C.c_int), ("reserved_i", C.c_int), ("device_ms", C.c_double),
                 ("min_cut_gap", C.c_double), ("svd_ms", C.c_double), ("svd_bytes", C.c_double),
                 ("svd_launches", C.c_longlong), ("svd_sweeps", C.c_longlong), ("kernel_launches", C.c_longlong),
-                ("svd_flops", C.c_double), ("reserved_d", C.c_double * 1)]
+                ("svd_flops", C.c_double), ("precond_ms", C.c_double)]
 
 
 _lib = None
@@ -106,6 +107,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.tessera_qa_session_run_host.restype = C.c_int
         L.tessera_qa_session_randomize.argtypes = [C.c_void_p, C.c_uint64]
         L.tessera_qa_session_randomize.restype = C.c_int
+        L.tessera_qa_session_randomize_graded.argtypes = [C.c_void_p, C.c_uint64, C.c_double]
+        L.tessera_qa_session_randomize_graded.restype = C.c_int
         L.tessera_qa_session_run.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t]
         L.tessera_qa_session_run.restype = C.c_int
         L.tessera_qa_session_stream.argtypes = [C.c_void_p]

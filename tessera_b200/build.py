@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtessera_qa.so")
-SOURCES = ["kernels.cu", "engine.cu", "noalloc.cu", "gnn.cu", "theta_tc.cu", "statevector.cu", "sa.cu"]
+SOURCES = ["kernels.cu", "engine.cu", "lq.cu", "noalloc.cu", "gnn.cu", "theta_tc.cu", "statevector.cu", "sa.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]
 

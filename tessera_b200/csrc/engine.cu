@@ -74,7 +74,7 @@ static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 __global__ void k_set_int(int* p, int v) { *p = v; }
 
 template <typename T>
-__global__ void k_random_sites(MpsView<T> mps, unsigned long long seed) {
+__global__ void k_random_sites(MpsView<T> mps, unsigned long long seed, double decay) {
     using V = cplx_t<T>;
     const int i = blockIdx.y;
     const int dl = mps.dims[i], dr = mps.dims[i + 1];
@@ -95,7 +95,9 @@ __global__ void k_random_sites(MpsView<T> mps, unsigned long long seed) {
         }
         const double u1 = ((u[0] >> 11) + 0.5) * (1.0 / 9007199254740992.0);
         const double u2 = (u[1] >> 11) * (1.0 / 9007199254740992.0);
-        const double r = sqrt(-2.0 * log(u1)) * scale;
+        // decay > 0: column b of every site scaled by exp(-b / decay), so that theta's singular
+        // values fall off like a TEBD state's Schmidt values instead of staying flat
+        const double r = sqrt(-2.0 * log(u1)) * scale * (decay > 0.0 ? exp(-(double)b / decay) : 1.0);
         S[row * mps.cap + b] = mk<V>((T)(r * cos(6.283185307179586 * u2)), (T)(r * sin(6.283185307179586 * u2)));
     }
 }
@@ -159,6 +161,7 @@ struct Config {
     int min_ld = 0;  // workspace rows/cols at least this (standalone SVD)
     int timing = 0;  // time each SVD launch with CUDA events
     int theta_tc = 0;  // complex64: bond contraction on tcgen05 tensor cores (split-TF32)
+    int precond = 0;   // batched column-pair Jacobi: 0 default (on), 1 on, 2 off (pivoted LQ first)
 };
 
 static Config validate_config(const tessera_qa_config* c) {
@@ -172,6 +175,7 @@ static Config validate_config(const tessera_qa_config* c) {
                              c->jacobi_block == 8 || c->jacobi_block == 16 || c->jacobi_block == 32))
         throw ArgError("jacobi_block must be 0, 1, 2, 4, 8, 16 or 32 (32: block-Gram Jacobi, batches only)");
     if (c->jacobi_max_sweeps < 0 || c->jacobi_max_sweeps > 1000) throw ArgError("jacobi_max_sweeps out of range");
+    if (c->jacobi_precondition < 0 || c->jacobi_precondition > 2) throw ArgError("jacobi_precondition must be 0, 1 or 2");
     C.dt = c->dt;
     C.ns = c->zz_substeps < 1 ? 1 : c->zz_substeps;
     C.precision = c->precision;
@@ -182,6 +186,7 @@ static Config validate_config(const tessera_qa_config* c) {
     C.device = c->device;
     C.timing = c->kernel_timing;
     C.theta_tc = c->theta_tensor_cores;
+    C.precond = c->jacobi_precondition;
     if (C.theta_tc && c->precision != TESSERA_QA_C64)
         throw ArgError("theta_tensor_cores needs complex64 precision");
     return C;
@@ -191,7 +196,7 @@ class EngineBase {
 public:
     virtual ~EngineBase() = default;
     virtual void init_plus() = 0;
-    virtual void randomize(unsigned long long seed) = 0;
+    virtual void randomize(unsigned long long seed, double decay) = 0;
     virtual void run(int k0, int k1) = 0;
     // gates [q0, q1) of the ZZ block of step k only (no single-site half steps, no entropy)
     virtual void run_gates(int k, int q0, int q1) = 0;
@@ -264,7 +269,7 @@ public:
         std::fill(ub_.begin(), ub_.end(), 1);
     }
 
-    void randomize(unsigned long long seed) override {
+    void randomize(unsigned long long seed, double decay) override {
         std::vector<int> d(n_ + 1, 1);
         for (int i = 1; i < n_; ++i) {
             long long a = 1, b = 1;
@@ -274,7 +279,7 @@ public:
         }
         TQ_CK(cudaMemcpyAsync(dims_, d.data(), sizeof(int) * (n_ + 1), cudaMemcpyHostToDevice, stream_));
         TQ_CK(cudaStreamSynchronize(stream_));
-        k_random_sites<T><<<dim3(64, n_), 256, 0, stream_>>>(mps(), seed);
+        k_random_sites<T><<<dim3(64, n_), 256, 0, stream_>>>(mps(), seed, decay);
         TQ_CK(cudaGetLastError());
         TQ_CK(cudaMemsetAsync(stats_, 0, sizeof(RunStats), stream_));
         ub_ = d;
@@ -884,7 +889,7 @@ class BatchBase {
 public:
     virtual ~BatchBase() = default;
     virtual int size() const = 0;
-    virtual void randomize(unsigned long long seed) = 0;
+    virtual void randomize(unsigned long long seed, double decay) = 0;
     virtual void run(int k0, int k1) = 0;
     virtual void run_gates(int k, int q0, int q1) = 0;
     virtual void set_values(const std::vector<ProblemHost>& P) = 0;
@@ -988,6 +993,7 @@ private:
         TQ_CK(cudaMemcpy(order_, order.data(), sizeof(int) * B, cudaMemcpyHostToDevice));
         resident_ = C[0].block == 0 && !C[0].theta_tc;
         theta_tc_ = C[0].theta_tc != 0;
+        precond_ = C[0].precond != 2;
         for (auto& e : eng_) TQ_CK(cudaStreamSynchronize(e->own_stream()));
     }
 
@@ -1002,8 +1008,8 @@ public:
     cudaStream_t stream() const override { return st_; }
     void set_timing(bool on) { timing_ = on; }
 
-    void randomize(unsigned long long seed) override {
-        for (size_t b = 0; b < eng_.size(); ++b) eng_[b]->randomize(seed + 7919ull * b);
+    void randomize(unsigned long long seed, double decay) override {
+        for (size_t b = 0; b < eng_.size(); ++b) eng_[b]->randomize(seed + 7919ull * b, decay);
         for (auto& e : eng_) TQ_CK(cudaStreamSynchronize(e->own_stream()));
     }
 
@@ -1037,6 +1043,12 @@ public:
             svd_ms_ += ms;
         }
         timed_.clear();
+        for (auto& pr : timed_lq_) {
+            float ms = 0;
+            TQ_CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+            lq_ms_ += ms;
+        }
+        timed_lq_.clear();
         pool_next_ = 0;
         if (!r) return;
         tessera_qa_result a;
@@ -1066,6 +1078,7 @@ public:
         r->svd_flops = a.svd_flops;
         r->svd_sweeps = a.svd_sweeps;
         r->svd_ms = svd_ms_;
+        r->precond_ms = lq_ms_;
         r->svd_launches = svd_launches_;
         r->kernel_launches = launches_;
         r->device_ms = ms_;
@@ -1104,6 +1117,8 @@ public:
                 throw;
             }
             TQ_CK(cudaStreamEndCapture(st_, &g));
+            graph_launches_ = launches_ - l0;  // kernels one replay launches
+            graph_svd_launches_ = svd_launches_ - s0;
             launches_ = l0;
             svd_launches_ = s0;
             graph_ = g;
@@ -1112,8 +1127,8 @@ public:
         for (int k = k0; k < k1; ++k) {
             if (graph) {
                 TQ_CK(cudaGraphLaunch(gexec_, st_));
-                launches_ += 4 + 4LL * q_max_;
-                svd_launches_ += q_max_;
+                launches_ += graph_launches_;
+                svd_launches_ += graph_svd_launches_;
             } else {
                 step_body(B);
             }
@@ -1139,15 +1154,18 @@ private:
     // gate slot q of every instance that has one: theta, Jacobi SVD, absorption
     void slot(int q) {
         const int nref = (int)(refs_off_[q + 1] - refs_off_[q]);
-        cudaEvent_t a = nullptr, b = nullptr;
+        cudaEvent_t a = nullptr, b = nullptr, c = nullptr, d = nullptr;
         if (timing_) {
             a = event();
             b = event();
+            c = event();
+            d = event();
         }
-        launch_update_batch<T>(insts_, refs_ + refs_off_[q], nref, cap_max_, 2 * cap_max_, block_, st_, a, b,
-                               theta_tc_);
+        const int nl = launch_update_batch<T>(insts_, refs_ + refs_off_[q], nref, cap_max_, 2 * cap_max_, block_,
+                                              st_, a, b, theta_tc_, precond_, c, d);
+        launches_ += nl;
         if (timing_) timed_.push_back({a, b});
-        launches_ += 4;
+        if (timing_ && nl == 5) timed_lq_.push_back({c, d});  // the preconditioner ran
         ++svd_launches_;
     }
     cudaEvent_t event() {
@@ -1159,9 +1177,9 @@ private:
         return e;
     }
     bool timing_ = false, ran_ = false;
-    double svd_ms_ = 0.0;
+    double svd_ms_ = 0.0, lq_ms_ = 0.0;
     long long svd_launches_ = 0;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timed_;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timed_, timed_lq_;
     std::vector<cudaEvent_t> pool_;
     size_t pool_next_ = 0;
 
@@ -1173,6 +1191,7 @@ private:
     cudaEvent_t e0_ = nullptr, e1_ = nullptr;
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t gexec_ = nullptr;
+    long long graph_launches_ = 0, graph_svd_launches_ = 0;
     char* base_ = nullptr;
     int* step_ = nullptr;
     InstTask<T>* insts_ = nullptr;
@@ -1181,6 +1200,7 @@ private:
     int *op_off_ = nullptr, *order_ = nullptr, *work_ = nullptr;
     bool resident_ = true;
     bool theta_tc_ = false;
+    bool precond_ = true;
     std::vector<size_t> refs_off_;
     int cap_max_ = 1, n_max_ = 1, q_max_ = 0, steps_ = 0, block_ = 8, rows_cap_ = 8;
     double ms_ = 0.0;
@@ -1494,10 +1514,15 @@ tessera_qa_session* tessera_qa_session_create_batch(const tessera_qa_problem* pr
 }
 
 int tessera_qa_session_randomize(tessera_qa_session* s, uint64_t seed) {
+    return tessera_qa_session_randomize_graded(s, seed, 0.0);
+}
+
+int tessera_qa_session_randomize_graded(tessera_qa_session* s, uint64_t seed, double decay) {
     return guarded([&]() -> int {
         if (!s) throw ArgError("session is NULL");
-        if (s->batch) s->batch->randomize(seed);
-        else s->eng->randomize(seed);
+        if (!(decay >= 0.0) || !std::isfinite(decay)) throw ArgError("decay must be a finite number >= 0");
+        if (s->batch) s->batch->randomize(seed, decay);
+        else s->eng->randomize(seed, decay);
         return 0;
     });
 }
@@ -1564,6 +1589,7 @@ int tessera_qa_session_sync(tessera_qa_session* s, tessera_qa_result* result) {
             result->device_ms = r.device_ms;
             result->min_cut_gap = r.min_cut_gap;
             result->svd_ms = r.svd_ms;
+            result->precond_ms = r.precond_ms;
             result->svd_bytes = r.svd_bytes;
             result->svd_flops = r.svd_flops;
             result->svd_launches = r.svd_launches;

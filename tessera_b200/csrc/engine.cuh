@@ -157,10 +157,16 @@ void launch_step_inc(int* step, cudaStream_t s);
 // batched launchers: `refs` selects (instance, gate) pairs; ub_* are upper bounds over the batch
 template <typename T>
 void launch_single_site_batch(const InstTask<T>* insts, int ninst, int n_max, int d2_ub_max, cudaStream_t s);
+// returns the number of kernels launched; precond: the pivoted LQ (lq.cu) before a column-pair
+// Jacobi of theta above 256 rows
 template <typename T>
-void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref, int d_ub, int rows_ub,
-                         int block_w, cudaStream_t s, cudaEvent_t svd_begin = nullptr,
-                         cudaEvent_t svd_end = nullptr, bool theta_tc = false);
+int launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref, int d_ub, int rows_ub,
+                        int block_w, cudaStream_t s, cudaEvent_t svd_begin = nullptr,
+                        cudaEvent_t svd_end = nullptr, bool theta_tc = false, bool precond = false,
+                        cudaEvent_t lq_begin = nullptr, cudaEvent_t lq_end = nullptr);
+// row-pivoted Householder LQ of each task's theta working copy, in place (lq.cu)
+template <typename T>
+void launch_lq_batch(const InstTask<T>* insts, const UpdRef* refs, int nref, cudaStream_t s);
 template <typename T>
 void launch_entropy_batch(const InstTask<T>* insts, int ninst, cudaStream_t s);
 // Whole anneal of every instance, one CTA per instance at a time (small bonds only); false

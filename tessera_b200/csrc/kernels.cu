@@ -1942,15 +1942,21 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
 }
 
 // Batched: each CTA takes whole SVD tasks (one theta each) in turn; no inter-CTA waits.
+// lq: W holds the pivoted LQ factor P L of theta (lq.cu), whose columns beyond min(R, N) are zero.
 template <typename T, int BW, int RPL>
 __global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd_batch(const InstTask<T>* insts, const UpdRef* refs,
-                                                                       int nref) {
+                                                                       int nref, int lq) {
     extern __shared__ __align__(16) unsigned char smraw[];
     for (int t = blockIdx.x; t < nref; t += gridDim.x) {
         const UpdRef rf = refs[t];
         const InstTask<T>& it = insts[rf.inst];
         SvdParams pp = it.pp;
         pp.bond = rf.op.bond;
+        if (lq && pp.R <= 0) {
+            pp.R = 2 * it.mps.dims[pp.bond];
+            const int n = 2 * it.mps.dims[pp.bond + 2];
+            pp.N = n < pp.R ? n : pp.R;
+        }
         if constexpr (RPL > 0) svd_body_rc<T, BW, RPL>(it.mps, it.wk, pp, smraw);
         else svd_body<T, BW, RPL>(it.mps, it.wk, pp, 0, 1, smraw);
         __syncthreads();
@@ -2508,7 +2514,8 @@ __global__ void __launch_bounds__(256) k_absorb_c_batch(const InstTask<T>* insts
 }
 
 template <typename T, int BW, int RPL>
-static void svd_batch_bw(const InstTask<T>* insts, const UpdRef* refs, int nref, int rows_cap, cudaStream_t s) {
+static void svd_batch_bw(const InstTask<T>* insts, const UpdRef* refs, int nref, int rows_cap, cudaStream_t s,
+                         int lq = 0) {
     using V = cplx_t<T>;
     constexpr int NT = SvdShape<BW, RPL>::NT;
     // block-row-cyclic (RPL > 0): block I plus two J buffers; else one staged block pair
@@ -2522,25 +2529,28 @@ static void svd_batch_bw(const InstTask<T>* insts, const UpdRef* refs, int nref,
     if (per_sm < 1) throw std::runtime_error("k_svd_batch does not fit on an SM");
     int grid = per_sm * num_sms();
     if (grid > nref) grid = nref;
-    fn<<<grid, NT, smem, s>>>(insts, refs, nref);
+    fn<<<grid, NT, smem, s>>>(insts, refs, nref, lq);
     TQ_CHECK(cudaGetLastError());
 }
 
 // complex64 at 512 rows: blocks of 16 columns (512 threads, 16 warps); a complex128 column pair
 // of 512 rows does not fit in the registers that 16 warps leave each thread
 template <typename T>
-static bool svd_batch_wide(const InstTask<T>* insts, const UpdRef* refs, int nref, int rows_cap, cudaStream_t s) {
+static bool svd_batch_wide(const InstTask<T>* insts, const UpdRef* refs, int nref, int rows_cap, cudaStream_t s,
+                           int lq) {
     if constexpr (sizeof(T) == 4) {
-        svd_batch_bw<T, 16, 16>(insts, refs, nref, rows_cap, s);
+        svd_batch_bw<T, 16, 16>(insts, refs, nref, rows_cap, s, lq);
         return true;
     }
     return false;
 }
 
 template <typename T>
-void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref, int d_ub, int rows_ub,
-                         int block_w, cudaStream_t s, cudaEvent_t svd_begin, cudaEvent_t svd_end, bool theta_tc) {
-    if (nref <= 0) return;
+int launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref, int d_ub, int rows_ub,
+                        int block_w, cudaStream_t s, cudaEvent_t svd_begin, cudaEvent_t svd_end, bool theta_tc,
+                        bool precond, cudaEvent_t lq_begin, cudaEvent_t lq_end) {
+    if (nref <= 0) return 0;
+    int launches = 4;
     if constexpr (sizeof(T) == 4) {
         if (theta_tc) {
             launch_theta_tc_batch(reinterpret_cast<const InstTask<float>*>(insts), refs, nref, d_ub, s);
@@ -2559,7 +2569,6 @@ void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref,
     if (rpl > 16 && block_w != BG_B) throw std::runtime_error("the column-pair batched SVD supports at most 512 rows");
     int bw = block_w < 4 ? 4 : block_w;
     if (rpl == 16 && bw > 8 && !(sizeof(T) == 4 && bw == 16)) bw = 8;
-    if (svd_begin) TQ_CHECK(cudaEventRecord(svd_begin, s));
     SvdParams rp{};
     rp.rows_cap = rows_cap;
     rp.cols_cap = rows_cap;  // every instance's theta is at most rows_ub x rows_ub
@@ -2567,13 +2576,23 @@ void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref,
     // one asked for; complex64 at 257..512 rows: 16), or the block-Gram kernel when block width
     // 32 is asked for
     if (block_w == 0) bw = (sizeof(T) == 4 && rpl == 16) ? 16 : 8;
+    // the pivoted LQ preconditioner for the column-pair kernel at 257..512 rows (outside the
+    // svd_begin/svd_end window, so that window times the Jacobi alone)
+    const int lq = (precond && block_w != BG_B && rpl == 16 && resident_smem<T>(rows_cap, rows_cap) == 0) ? 1 : 0;
+    if (lq) {  // lq_begin/lq_end are recorded only here: a return of 5 launches says they were
+        if (lq_begin) TQ_CHECK(cudaEventRecord(lq_begin, s));
+        launch_lq_batch<T>(insts, refs, nref, s);
+        if (lq_end) TQ_CHECK(cudaEventRecord(lq_end, s));
+        ++launches;
+    }
+    if (svd_begin) TQ_CHECK(cudaEventRecord(svd_begin, s));
     if (res_dispatch<T>(nullptr, nullptr, rp, insts, refs, nref, s)) {
     } else if (block_w == BG_B) {
         bgj_launch<T>(nullptr, nullptr, nullptr, insts, refs, nref, s);
-    } else if (bw == 16 && rpl == 16 && svd_batch_wide<T>(insts, refs, nref, rows_cap, s)) {
+    } else if (bw == 16 && rpl == 16 && svd_batch_wide<T>(insts, refs, nref, rows_cap, s, lq)) {
     } else {
 #define TQ_RB(B, RP) \
-    if (bw == B && rpl == RP) { svd_batch_bw<T, B, RP>(insts, refs, nref, rows_cap, s); } else
+    if (bw == B && rpl == RP) { svd_batch_bw<T, B, RP>(insts, refs, nref, rows_cap, s, lq); } else
         TQ_RB(4, 1) TQ_RB(4, 2) TQ_RB(4, 4) TQ_RB(4, 8) TQ_RB(4, 16)
         TQ_RB(8, 1) TQ_RB(8, 2) TQ_RB(8, 4) TQ_RB(8, 8) TQ_RB(8, 16)
         TQ_RB(16, 1) TQ_RB(16, 2) TQ_RB(16, 4) TQ_RB(16, 8)
@@ -2586,6 +2605,7 @@ void launch_update_batch(const InstTask<T>* insts, const UpdRef* refs, int nref,
     TQ_CHECK(cudaGetLastError());
     k_absorb_c_batch<T><<<dim3((2 * d_ub + 31) / 32, keep_tiles, nref), 256, 0, s>>>(insts, refs);
     TQ_CHECK(cudaGetLastError());
+    return launches;
 }
 
 // One CTA per instance: right-environment chain to bond 1, then the qubit-0 entropy.
@@ -2626,8 +2646,8 @@ void launch_entropy_batch(const InstTask<T>* insts, int ninst, cudaStream_t s) {
                                       cudaStream_t);                                                        \
     template void launch_amplitude<T>(const MpsView<T>&, const int8_t*, cplx_t<T>*, double*, cudaStream_t);   \
     template void launch_single_site_batch<T>(const InstTask<T>*, int, int, int, cudaStream_t);                \
-    template void launch_update_batch<T>(const InstTask<T>*, const UpdRef*, int, int, int, int, cudaStream_t,  \
-                                         cudaEvent_t, cudaEvent_t, bool);                                    \
+    template int launch_update_batch<T>(const InstTask<T>*, const UpdRef*, int, int, int, int, cudaStream_t,   \
+                                        cudaEvent_t, cudaEvent_t, bool, bool, cudaEvent_t, cudaEvent_t);     \
     template void launch_entropy_batch<T>(const InstTask<T>*, int, cudaStream_t);                               \
     template void launch_sample<T>(const MpsView<T>&, const cplx_t<T>*, int, unsigned long long, int8_t*,       \
                                    cudaStream_t);                                                              \

@@ -142,7 +142,9 @@ def problem_struct(h, ei, ej, ew, sa, sb, bias=None, sc=None):
 
 def config_struct(dt=0.1, chi=32, precision="c128", zz_substeps=1, jacobi_tol=0.0, jacobi_max_sweeps=0,
                   jacobi_block=0, device=-1, step_begin=0, step_end=0, initial_mps=None, skip_observables=False,
-                  theta_tensor_cores=False):
+                  theta_tensor_cores=False, jacobi_precondition=0):
+    """jacobi_precondition: 0 default (on), 1 on, 2 off -- the pivoted LQ before the batched
+    column-pair Jacobi of theta above 256 rows."""
     L = _lib.load()
     c = _lib.Config()
     L.tessera_qa_config_init(C.byref(c))
@@ -165,6 +167,7 @@ def config_struct(dt=0.1, chi=32, precision="c128", zz_substeps=1, jacobi_tol=0.
         c.initial_mps = keep.ctypes.data
     c.skip_observables = 1 if skip_observables else 0
     c.theta_tensor_cores = 1 if theta_tensor_cores else 0
+    c.jacobi_precondition = int(jacobi_precondition)
     return c, keep
 
 
@@ -340,8 +343,13 @@ class Session:
         if rc != 0:
             raise _lib.EngineError(rc, _lib.last_error())
 
-    def randomize(self, seed: int):
-        self._ck(self._L.tessera_qa_session_randomize(self._h, seed))
+    def randomize(self, seed: int, decay: float = 0.0):
+        """Seeded random MPS with every bond at its cap; decay > 0 grades each theta's spectrum
+        (site column b scaled by exp(-b / decay))."""
+        if decay:
+            self._ck(self._L.tessera_qa_session_randomize_graded(self._h, seed, float(decay)))
+        else:
+            self._ck(self._L.tessera_qa_session_randomize(self._h, seed))
 
     def run(self, step_begin: int, nsteps: int):
         self._ck(self._L.tessera_qa_session_run(self._h, step_begin, nsteps))

@@ -79,6 +79,40 @@ def one_sided_jacobi(A: np.ndarray, rule: str = "A", tol: float = 1e-13, max_swe
     return sig[order], W[:, order], sweeps, float(np.sqrt(tiny))
 
 
+def pivoted_lq(A: np.ndarray) -> np.ndarray:
+    """The preconditioner of tessera_b200/csrc/lq.cu, step for step: a row-pivoted Householder LQ
+    P^T A = L Q^H returned as P L in A's own row order.  Step k takes the unpivoted row of largest
+    remaining norm (downdated by its new column-k entry, recomputed exactly in each pass), forms
+    the reflector u = x with u_0 = e (|x_0| + alpha), tau = 1/(alpha (alpha + |x_0|)) from that row
+    x = X[p, k:], sets X[p, k] = -e alpha and zeroes the rest of the row, and updates every other
+    unpivoted row z <- z - tau (z . conj(u)) u.  The kernel folds the update of the next pivot row
+    into its reflector and fuses each update with the next step's products; the arithmetic is the
+    same."""
+    X = np.array(A, dtype=np.complex128, copy=True)
+    R, N = X.shape
+    nrm = np.sum(np.abs(X) ** 2, axis=1)
+    free = np.ones(R, bool)
+    for k in range(min(R, N)):
+        key = np.where(free, nrm, -1.0)
+        p = int(np.flatnonzero(key == key.max())[0])
+        x = X[p, k:].copy()
+        alpha, a0 = np.sqrt(np.sum(np.abs(x) ** 2)), abs(x[0])
+        e = x[0] / a0 if a0 > 0 else 1.0
+        free[p] = False
+        X[p, k:] = 0
+        if alpha == 0:
+            continue
+        X[p, k] = -e * alpha
+        u = x.copy()
+        u[0] = e * (a0 + alpha)
+        tau = 1.0 / (alpha * (alpha + a0))
+        rows = np.flatnonzero(free)
+        w = X[rows, k:] @ np.conj(u)
+        X[rows, k:] -= tau * np.outer(w, u)
+        nrm[rows] = np.maximum(0.0, nrm[rows] - np.abs(X[rows, k]) ** 2)
+    return X
+
+
 def graded(n: int, decay: float, seed: int) -> tuple[np.ndarray, np.ndarray]:
     """n x n matrix U diag(exp(-k/decay)) V^H with Haar-like random unitary U, V."""
     rng = np.random.Generator(np.random.PCG64(seed))

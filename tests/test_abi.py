@@ -165,6 +165,7 @@ def test_null_handles_and_structs_are_rejected_without_a_gpu():
     f0 = C.c_float(0.0)
     einval = {
         "session_randomize": lambda: L.tessera_qa_session_randomize(None, 1),
+        "session_randomize_graded": lambda: L.tessera_qa_session_randomize_graded(None, 1, 24.0),
         "session_run": lambda: L.tessera_qa_session_run(None, 0, 1),
         "session_run_gates": lambda: L.tessera_qa_session_run_gates(None, 0, 0, 1),
         "session_run_host": lambda: L.tessera_qa_session_run_host(None, None, 0, 0, 0, 0, None),

@@ -8,7 +8,7 @@ sweep still rotates >= 10% of its pairs, then rule A) resolves them at the same 
 import numpy as np
 import pytest
 
-from jacobi_model import graded, one_sided_jacobi
+from jacobi_model import graded, one_sided_jacobi, pivoted_lq
 
 
 @pytest.fixture(scope="module")
@@ -52,3 +52,37 @@ def test_model_rotation_matches_the_textbook_form():
         t = np.sign(zeta if zeta != 0 else 1.0) / (abs(zeta) + np.sqrt(1 + zeta * zeta))
         assert c == pytest.approx(1 / np.sqrt(1 + t * t), rel=1e-14)
         assert s == pytest.approx(t / np.sqrt(1 + t * t), rel=1e-13, abs=1e-300)
+
+
+def test_pivoted_lq_preconditioner_cuts_sweeps_on_a_graded_spectrum():
+    """The batched Jacobi's preconditioner (lq.cu): P L equals A times a unitary (so the Jacobi on it
+    gives A's singular values and, as W / sigma, A's left singular vectors in A's row order), L is
+    lower trapezoidal in pivot order, and on a graded spectrum (values falling by 1e-10 over 96
+    columns) the Jacobi on P L takes far fewer sweeps than on A."""
+    A, s = graded(96, 4.0, 11)
+    X = pivoted_lq(A)
+    assert np.linalg.norm(X @ X.conj().T - A @ A.conj().T) < 1e-14 * np.linalg.norm(A) ** 2
+    # row-pivot order: each row of P L has at most one more nonzero than the one pivoted before it
+    nnz = sorted(int(np.max(np.flatnonzero(np.abs(r) > 0))) + 1 for r in X if np.any(np.abs(r) > 0))
+    assert nnz == list(range(1, len(nnz) + 1))
+    sig_a, _, sweeps_a, floor = one_sided_jacobi(A, "F")
+    sig_x, W, sweeps_x, _ = one_sided_jacobi(X, "F")
+    # absolute accuracy under the noise floor, as good as the Jacobi on A itself
+    assert np.max(np.abs(sig_x - s)) < floor
+    assert np.max(np.abs(sig_x - s)) <= 2 * np.max(np.abs(sig_a - s))
+    assert sweeps_x * 2 <= sweeps_a, (sweeps_x, sweeps_a)  # observed 6 against 16
+    # U = W / sigma spans A's leading left singular subspace
+    U = W[:, :8] / sig_x[:8]
+    Ua = np.linalg.svd(A)[0][:, :8]
+    assert np.linalg.norm(Ua.conj().T @ U, 2) == pytest.approx(1.0, abs=1e-10)
+    assert np.linalg.svd(Ua.conj().T @ U, compute_uv=False).min() > 1 - 1e-10
+
+
+def test_pivoted_lq_of_wide_and_tall_matrices():
+    rng = np.random.default_rng(5)
+    for R, N in ((24, 40), (40, 24)):
+        A = rng.normal(size=(R, N)) + 1j * rng.normal(size=(R, N))
+        X = pivoted_lq(A)
+        assert np.linalg.norm(X @ X.conj().T - A @ A.conj().T) < 1e-13 * np.linalg.norm(A) ** 2
+        if N > R:
+            assert np.all(X[:, R:] == 0)  # the Jacobi runs on min(R, N) columns
