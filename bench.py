@@ -453,7 +453,9 @@ def main():
         from tessera_b200 import autotune
         ch = autotune.tune(probs, args.chi, args.precision)
         args.jacobi_block, args.theta_tc = ch.jacobi_block, ch.theta_tensor_cores
+        args.precondition = "on" if ch.jacobi_precondition == 1 else "off"
         tuned = {"jacobi_block": ch.jacobi_block, "theta_tensor_cores": ch.theta_tensor_cores,
+                 "jacobi_precondition": args.precondition,
                  "measured_ms_per_update": {k: v["ms_per_update"] for k, v in ch.measured.items()}}
     upd_per_step_inst = min(args.gates, p.updates_per_step())
     if B == 1:

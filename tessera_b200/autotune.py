@@ -1,9 +1,10 @@
 """Measured choice of the batched Jacobi kernel for a workload (the engine's autotuner).
 
 The batched engine has three SVD kernels for a large theta (the block-row-cyclic column-pair
-Jacobi with blocks of 4 or 8 columns, and the block-Gram Jacobi) and, for complex64, two bond
-contractions (CUDA cores or tcgen05 tensor cores).  Which is fastest depends on the bond
-dimension, the precision and how many instances share the GPU.  ``tune`` times each candidate
+Jacobi with blocks of 4 or 8 columns, and the block-Gram Jacobi), the column-pair Jacobi with or
+without its pivoted-LQ preconditioner, and, for complex64, two bond contractions (CUDA cores or
+tcgen05 tensor cores).  Which is fastest depends on the bond dimension, the precision, the
+spectra and how many instances share the GPU.  ``tune`` times each candidate
 on the workload itself: a batched session of the given instances, each MPS a seeded random state
 with every bond at its cap, a few interior gate slots per candidate, CUDA events around them.
 The choice is cached in a JSON file keyed by (chi, precision, instance count, GPU name), so a
@@ -30,6 +31,7 @@ class Choice:
     theta_tensor_cores: bool
     ms_per_update: float
     measured: dict
+    jacobi_precondition: int = 1  # 1 on, 2 off (tessera_qa_config.jacobi_precondition)
 
 
 def _gpu_name() -> str:
@@ -41,14 +43,17 @@ def _gpu_name() -> str:
 
 
 def candidates(precision: str):
-    out = [(8, False), (4, False), (32, False)]
+    """(jacobi_block, theta_tensor_cores, jacobi_precondition) triples; the block-Gram kernel (32)
+    takes no preconditioner."""
+    out = [(8, False, 1), (8, False, 2), (4, False, 1), (32, False, 2)]
     if precision == "c64":
-        out += [(16, False), (8, True)]
+        out += [(16, False, 1), (16, False, 2), (16, True, 1)]
     return out
 
 
-def _time_candidate(problems, chi, precision, block, tc, q0, gates, seed=1234):
-    s = ffi.Session.batch(problems, chi=chi, precision=precision, jacobi_block=block, theta_tensor_cores=tc)
+def _time_candidate(problems, chi, precision, block, tc, q0, gates, seed=1234, precond=1):
+    s = ffi.Session.batch(problems, chi=chi, precision=precision, jacobi_block=block, theta_tensor_cores=tc,
+                          jacobi_precondition=precond)
     try:
         s.randomize(seed)
         k = problems[0].steps // 2
@@ -65,8 +70,9 @@ def _time_candidate(problems, chi, precision, block, tc, q0, gates, seed=1234):
 
 def tune(problems, chi: int, precision: str = "c128", gates: int = 2, q0: int | None = None, cache: str | None = CACHE,
          force: bool = False) -> Choice:
-    """Fastest (jacobi_block, theta_tensor_cores) for a batched run of `problems` at bond cap `chi`."""
-    key = f"chi={chi}|{precision}|B={len(problems)}|{_gpu_name()}"
+    """Fastest (jacobi_block, theta_tensor_cores, jacobi_precondition) for a batched run of
+    `problems` at bond cap `chi`."""
+    key = f"chi={chi}|{precision}|B={len(problems)}|{_gpu_name()}|lq"
     if cache and not force and os.path.exists(cache):
         try:
             with open(cache) as f:
@@ -82,17 +88,17 @@ def tune(problems, chi: int, precision: str = "c128", gates: int = 2, q0: int | 
     q0 = max(0, min(q0, ups - 1 - gates))
     gates = min(gates, ups - 1 - q0)
     measured = {}
-    for block, tc in candidates(precision):
+    for block, tc, pc in candidates(precision):
         t0 = time.perf_counter()
-        ms = _time_candidate(problems, chi, precision, block, tc, q0, gates)
-        measured[f"block={block},tc={int(tc)}"] = {"ms_per_update": ms, "wall_s": time.perf_counter() - t0}
+        ms = _time_candidate(problems, chi, precision, block, tc, q0, gates, precond=pc)
+        measured[f"block={block},tc={int(tc)},lq={int(pc == 1)}"] = {"ms_per_update": ms,
+                                                                   "wall_s": time.perf_counter() - t0}
     ok = {k: v["ms_per_update"] for k, v in measured.items() if v["ms_per_update"] is not None}
     if not ok:
         raise RuntimeError("no Jacobi kernel candidate ran cleanly on this workload")
     best = min(ok, key=ok.get)
-    block = int(best.split(",")[0].split("=")[1])
-    tc = best.endswith("tc=1")
-    choice = Choice(block, tc, ok[best], measured)
+    f = dict(kv.split("=") for kv in best.split(","))
+    choice = Choice(int(f["block"]), f["tc"] == "1", ok[best], measured, 1 if f["lq"] == "1" else 2)
     if cache:
         try:
             os.makedirs(os.path.dirname(cache), exist_ok=True)

@@ -42,6 +42,7 @@ namespace tq {
 
 constexpr int LQ_NT = 512;     // threads per CTA: one per row of theta
 constexpr int LQ_MAXN = 1024;  // columns of theta
+constexpr int LQ_U = 4;        // columns per chunk of the per-row walk
 
 __device__ __forceinline__ double2 to_d2(const double2 v) { return v; }
 __device__ __forceinline__ double2 to_d2(const float2 v) { return make_double2(v.x, v.y); }
@@ -203,13 +204,25 @@ __device__ void lq_body(cplx_t<T>* W, const int ld, const int R, const int N, in
                 acc.y += zd.y * un.x - zd.x * un.y;
                 nz += zd.x * zd.x + zd.y * zd.y;
             };
+            // columns in chunks of LQ_U, the loads of the next chunk issued before the current one
+            // is applied and stored, so two chunks of memory latency overlap per thread
             int c = k + 1;
-            for (; c + 4 <= N; c += 4) {
-                V xv[4];
+            const int nfull = (N - c) / LQ_U;
+            if (nfull > 0) {
+                V cur[LQ_U];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) xv[j] = row[(long long)(c + j) * ld];
+                for (int j = 0; j < LQ_U; ++j) cur[j] = row[(long long)(c + j) * ld];
+                for (int it = 0; it < nfull; ++it, c += LQ_U) {
+                    V nxt[LQ_U];
+                    if (it + 1 < nfull) {
 #pragma unroll
-                for (int j = 0; j < 4; ++j) step(xv[j], c + j);
+                        for (int j = 0; j < LQ_U; ++j) nxt[j] = row[(long long)(c + LQ_U + j) * ld];
+                    }
+#pragma unroll
+                    for (int j = 0; j < LQ_U; ++j) step(cur[j], c + j);
+#pragma unroll
+                    for (int j = 0; j < LQ_U; ++j) cur[j] = nxt[j];
+                }
             }
             for (; c < N; ++c) step(row[(long long)c * ld], c);
             w = acc;
