@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--graded-decay", type=float, default=24.0,
                     help="also time the step on random MPS with graded spectra (site column b scaled by "
                          "exp(-b/decay)); 0 = skip")
+    ap.add_argument("--no-c64", action="store_true", help="skip the complex64 leg of a complex128 run")
     ap.add_argument("--precondition", choices=["on", "off"], default="on",
                     help="pivoted LQ of theta before the batched Jacobi (fewer sweeps)")
     ap.add_argument("--theta-tc", action="store_true",
@@ -348,6 +349,67 @@ def plain_rate(args, local, peak_gbs=None, peak_tflops=None):
     return g / (r.device_ms / 1e3), r.device_ms / g, roof
 
 
+def c64_leg(args, probs, window, rank, world, local, peak_gbs):
+    """The same timed step in complex64 (FP32 storage and rotations, FP64 reductions): the same
+    instances, random start, warm-up and timed gate windows, on a complex64 batched session.
+    Returns its updates/s over all ranks (device time, max over ranks), its Jacobi sweeps and
+    the roofline of its Jacobi kernel against the FP32 GEMM rate measured here."""
+    import torch
+    import torch.distributed as dist
+    from tessera_b200 import ffi
+    sess = ffi.Session.batch(probs, chi=args.chi, precision="c64", kernel_timing=True, device=local,
+                             jacobi_precondition=1 if args.precondition == "on" else 2)
+    try:
+        sess.randomize(1234 + 1000 * rank)
+        for w in range(args.warmup):
+            q0, q1 = window(w)
+            sess.run_gates(MID_STEP, q0, q1)
+        r0 = sess.sync()
+        stream = torch.cuda.ExternalStream(sess.stream)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(args.steps):
+            q0, q1 = window(args.warmup + k)
+            sess.run_gates(MID_STEP, q0, q1)
+        e1.record(stream)
+        r1 = sess.sync()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1), world)
+        st = job_status(r1.status, world)
+        if st:
+            raise RuntimeError(f"engine status bits {st} in the complex64 steps (largest over ranks)")
+    finally:
+        sess.close()
+    upd = r1.two_site_updates - r0.two_site_updates
+    n = max(r1.svd_launches - r0.svd_launches, 1)
+    svd_ms = r1.svd_ms - r0.svd_ms
+    flops = r1.svd_flops - r0.svd_flops
+    byts = r1.svd_bytes - r0.svd_bytes
+    try:
+        p32 = fp64_peak_tflops(torch.float32)
+    except Exception:
+        p32 = None
+    ach = flops / (svd_ms / 1e3) / 1e12 if svd_ms else 0.0
+    gbs = byts / (svd_ms / 1e3) / 1e9 if svd_ms else 0.0
+    return {"value": upd * world / (ms / 1e3), "unit": UNIT, "dtype": "f32", "ms_per_step": ms / args.steps,
+            "avg_sweeps": (r1.svd_sweeps - r0.svd_sweeps) / max(upd, 1),
+            "precond_avg_launch_ms": (r1.precond_ms - r0.precond_ms) / n,
+            "roofline": {"kernel": "k_svd_batch (complex64 column-pair Jacobi in blocks of 16)", "bound": "fp32",
+                         "achieved": ach, "peak": p32, "unit": "TFLOP/s", "frac": ach / p32 if p32 else None,
+                         "peak_kind": "cuBLAS SGEMM 4096^3 measured in this run (best of 5)",
+                         "avg_launch_ms": svd_ms / n, "hbm_achieved_gbs": gbs,
+                         "hbm_frac": gbs / peak_gbs if peak_gbs else None},
+            "workload": "the headline's instances, random start, warm-up and timed gate windows in complex64 "
+                        "(FP32 storage, contraction and rotations; FP64 convergence test, discarded weight, "
+                        "entropy and norms)"}
+
+
 def solves(args):
     """Second half of the metric: solves/s at <= 1% energy gap, chosen vs plain.
 
@@ -561,13 +623,16 @@ def main():
                         "flops_per_launch": svd_flops / max(svd_n, 1)}
 
     # the pivoted-LQ preconditioner (k_lq_batch): its own launches, timed apart from the Jacobi;
-    # algorithmic bytes per theta: two reads of theta (row norms, first products), then per
-    # elimination step one read and one write of the trailing block
+    # algorithmic bytes per theta: one read for the row norms, then per elimination step one read
+    # of the trailing block and one write of column k, and per panel of 8 steps one read and one
+    # write of the trailing block (the delayed updates)
     precond = None
     if B > 1 and args.precondition == "on" and lq_ms > 0:
         R = Nc = 2 * args.chi
         esz = 16 if args.precision == "c128" else 8
-        lq_bytes = esz * (2 * R * Nc + 2 * sum((R - k) * (Nc - k) for k in range(min(R, Nc))))
+        km = min(R, Nc)
+        lq_bytes = esz * (R * Nc + sum((R - k) * (Nc - k) + (R - k) for k in range(km))
+                          + sum(2 * (R - k) * (Nc - k) for k in range(8, km + 1, 8)))
         lq_per_launch = B * lq_bytes
         lq_avg = lq_ms / max(svd_n, 1)
         precond = {"kernel": "k_lq_batch (row-pivoted Householder LQ, one CTA per 512x512 theta)",
@@ -645,9 +710,16 @@ def main():
                               "values fall off like a TEBD state's Schmidt values (the 256th ~1e-7 of the largest "
                               "before the gate) instead of staying flat"}
 
+    c64_line = None
+    if B > 1 and args.precision == "c128" and not args.no_c64:
+        sess.close()  # the complex64 session takes the memory the complex128 one held
+        sess = None
+        c64_line = c64_leg(args, probs, window, rank, world, local, peak)
+
     plain = None
     if B > 1 and rank == 0:
-        sess.close()
+        if sess is not None:
+            sess.close()
         try:
             pr, pms, proof = plain_rate(args, local, peak, p64)
             plain = {"value": pr, "unit": UNIT, "ms_per_update": pms,
@@ -686,13 +758,13 @@ def main():
                 "data": "synthetic: seeded Ising instances (PCG64 seeds 2..) and seeded random MPS with every "
                         "bond at its cap",
                 "config": cfg, "roofline": roofline, "compute_roofline": compute_roofline, "preconditioner": precond,
-                "graded_spectra": graded,
+                "graded_spectra": graded, "complex64": c64_line,
                 "cpu_baseline": cpu,
                 "e2e": e2e,
                 "gpu_launches": launches, "clocks": ck, "plain_single_instance": plain, "solves": sol,
                 "max_trunc_in_timed_steps": r1.max_trunc}
         print(json.dumps(line))
-    if B == 1 or rank != 0:
+    if sess is not None and (B == 1 or rank != 0):
         sess.close()
     if world > 1:
         dist.destroy_process_group()

@@ -20,11 +20,13 @@
 //     x = X[p, k:],  alpha = ||x||,  e = x_0 / |x_0|,
 //     u = x with u_0 = e (|x_0| + alpha),  tau = 1 / (alpha (alpha + |x_0|)),
 //     x (I - tau u^H u) = -e alpha e_0      (row vectors; I - tau u^H u is Hermitian unitary),
-// and applies it to every other unpivoted row z:  z <- z - tau (z . conj(u)) u.  The products
-// w_i = X[i, k:] . conj(u) of all rows are accumulated in the same pass that applies the
-// previous step's reflector, so each step reads and writes the trailing block once.  Row norms
-// are downdated by the new column-k entry before the pivot search and recomputed exactly in
-// the next pass.  All sums (w, norms, alpha) are FP64; complex64 stores in FP32.
+// and applies it to every other unpivoted row z:  z <- z - tau (z . conj(u)) u.  The updates
+// are delayed over panels of LQ_B steps (the blocking of LAPACK's pivoted QR): a step reads the
+// trailing block once for the products w_i = X[i, k:] . conj(u), corrects them for the panel's
+// pending updates, and writes only column k; the panel's updates reach memory in one pass at its
+// end.  Per step that moves (1 + 2/LQ_B) instead of 2 trailing blocks.  Row norms are downdated
+// by the new column-k entry before each pivot search and recomputed exactly at panel ends.  All
+// sums (w, norms, alpha) are FP64; complex64 stores in FP32.
 #include <stdexcept>
 #include <string>
 
@@ -43,6 +45,7 @@ namespace tq {
 constexpr int LQ_NT = 512;     // threads per CTA: one per row of theta
 constexpr int LQ_MAXN = 1024;  // columns of theta
 constexpr int LQ_U = 4;        // columns per chunk of the per-row walk
+constexpr int LQ_B = 8;        // reflectors per panel (delayed updates)
 
 __device__ __forceinline__ double2 to_d2(const double2 v) { return v; }
 __device__ __forceinline__ double2 to_d2(const float2 v) { return make_double2(v.x, v.y); }
@@ -83,160 +86,199 @@ __device__ __forceinline__ double block_sum(double v, double* rv) {
     return s;
 }
 
-// In-place pivoted LQ of W (R x N, column-major, ld): W <- P L (see the file comment).
+// sum of up to LQ_RED doubles v[0..n) over the CTA into out[0..n) (every thread may read out after)
+constexpr int LQ_RED = 2 * LQ_B;
+__device__ __forceinline__ void block_sum_n(double* v, int n, double (*red)[LQ_RED], double* out) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    for (int q = 0; q < n; ++q) {
+        const double s = warp_sum(v[q]);
+        if (lane == 0) red[warp][q] = s;
+    }
+    __syncthreads();
+    if (tid < n) {
+        double s = 0.0;
+        for (int w = 0; w < nw; ++w) s += red[w][tid];
+        out[tid] = s;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ double2 cm(const double2 a, const double2 b) {  // a * b
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cmc(const double2 a, const double2 b) {  // a * conj(b)
+    return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+// In-place pivoted LQ of W (R x N, column-major, ld): W <- P L (see the file comment).  Panels
+// of LQ_B steps: within a panel the trailing block in memory is not updated; row i's current
+// values are X[i, c] - sum_j tw_j[i] u_j[c] over the panel's reflectors so far (tw_j[i] =
+// tau_j w_j[i]), so each step reads the trailing block once (its products with the new
+// reflector, corrected by g_j = u_j . conj(u)), writes only column k, and the panel's updates
+// are written in one pass at its end, where the row norms are also recomputed exactly.
 template <typename T>
 __device__ void lq_body(cplx_t<T>* W, const int ld, const int R, const int N, int* status, unsigned char* smraw) {
     using V = cplx_t<T>;
     __shared__ double rv[LQ_NT / 32];
     __shared__ int ri[LQ_NT / 32];
+    __shared__ double red[LQ_NT / 32][LQ_RED];
+    __shared__ double s_red[LQ_RED];
     __shared__ double s_tau;
-    __shared__ double2 s_d, s_tw;
+    __shared__ double2 s_d;
     const int tid = threadIdx.x;
     if (R > (int)blockDim.x || N > LQ_MAXN || R < 1 || N < 1) {  // host sizing bug guard
         if (tid == 0) atomicOr(status, ST_BAD_DIMS);
         return;
     }
-    double2* ucur = reinterpret_cast<double2*>(smraw);  // reflector of the current step [LQ_MAXN]
-    double2* unext = ucur + LQ_MAXN;                    // reflector of the next step
+    double2* U = reinterpret_cast<double2*>(smraw);  // [LQ_B][LQ_MAXN] the panel's reflectors
+    double2* TW = U + LQ_B * LQ_MAXN;                 // [LQ_B][LQ_NT] tau_j w_j of every row
     const int kmax = R < N ? R : N;
     const bool mine = tid < R;
     bool pivoted = !mine;
-
-    // Reflector of step k from row p into u (columns >= k): x[c] = X[p, c] - tw uprev[c], where
-    // tw uprev is the previous step's update of row p, not yet written; sets s_tau and s_d (the
-    // diagonal entry of L).
-    auto form = [&](const int k, const int p, const double2 tw, const double2* uprev, double2* u) {
-        double part = 0.0;
-        for (int c = k + tid; c < N; c += blockDim.x) {
-            double2 x = to_d2(W[p + (long long)c * ld]);
-            if (uprev) {
-                const double2 q = uprev[c];
-                x.x -= tw.x * q.x - tw.y * q.y;
-                x.y -= tw.x * q.y + tw.y * q.x;
-            }
-            u[c] = x;
-            part += x.x * x.x + x.y * x.y;
-        }
-        const double alpha2 = block_sum(part, rv);  // ends with a barrier: u complete
-        if (tid == 0) {
-            const double alpha = sqrt(alpha2);
-            const double2 x0 = u[k];
-            const double a0 = sqrt(x0.x * x0.x + x0.y * x0.y);
-            const double ex = a0 > 0.0 ? x0.x / a0 : 1.0, ey = a0 > 0.0 ? x0.y / a0 : 0.0;
-            if (alpha > 0.0) {
-                s_d = make_double2(-ex * alpha, -ey * alpha);
-                s_tau = 1.0 / (alpha * (alpha + a0));
-                u[k] = make_double2(ex * (a0 + alpha), ey * (a0 + alpha));
-            } else {  // the rest of theta is zero: the identity
-                s_d = make_double2(0.0, 0.0);
-                s_tau = 0.0;
-            }
-        }
-        __syncthreads();
-    };
-
-    // exact row norms, the first pivot and its reflector
+    V* row = W + tid;
+    // exact row norms
     double nrm = 0.0;
     if (mine)
         for (int c = 0; c < N; ++c) {
-            const double2 x = to_d2(W[tid + (long long)c * ld]);
+            const double2 x = to_d2(row[(long long)c * ld]);
             nrm += x.x * x.x + x.y * x.y;
         }
-    int p = block_argmax(mine ? nrm : -1.0, rv, ri);
-    form(0, p, make_double2(0.0, 0.0), nullptr, ucur);
-    double tau = s_tau;
-    double2 d = s_d;
-    // w_i = X[i, 0:] . conj(u_0)
-    double2 w = make_double2(0.0, 0.0);
-    if (mine && tid != p)
-        for (int c = 0; c < N; ++c) {
-            const double2 x = to_d2(W[tid + (long long)c * ld]);
-            const double2 q = ucur[c];
-            w.x += x.x * q.x + x.y * q.y;
-            w.y += x.y * q.x - x.x * q.y;
-        }
-
-    for (int k = 0; k < kmax; ++k) {
-        // column k: the pivot row takes its diagonal entry of L, every other unpivoted row the
-        // update of step k; the norms of columns > k follow by downdating
-        if (tid == p) {
-            W[p + (long long)k * ld] = from_d2<V>(d);
-            pivoted = true;
-        } else if (!pivoted) {
-            const double2 x = to_d2(W[tid + (long long)k * ld]);
-            const double2 q = ucur[k];
-            const double twx = tau * w.x, twy = tau * w.y;
-            const V a = from_d2<V>(make_double2(x.x - (twx * q.x - twy * q.y), x.y - (twx * q.y + twy * q.x)));
-            W[tid + (long long)k * ld] = a;
-            const double2 ad = to_d2(a);
-            nrm = fmax(0.0, nrm - (ad.x * ad.x + ad.y * ad.y));
-        }
-        if (k + 1 == kmax) {
-            // last step: a wide theta's last pivot row is zero right of the diagonal
-            if (tid == p)
-                for (int c = k + 1; c < N; ++c) W[p + (long long)c * ld] = czero<V>();
-            break;
-        }
-        __syncthreads();
-        const int pn = block_argmax(pivoted ? -1.0 : nrm, rv, ri);
-        if (tid == pn) s_tw = make_double2(tau * w.x, tau * w.y);
-        __syncthreads();
-        // the next pivot row, brought up to date by step k on the fly, gives the next reflector
-        form(k + 1, pn, s_tw, ucur, unext);
-        // one pass over the columns > k: apply step k's reflector to every unpivoted row but the
-        // next pivot (its update is folded into its reflector), accumulating step k+1's
-        // products and the exact remaining norms; the row pivoted at step k is zeroed there
-        if (tid == p) {
-            for (int c = k + 1; c < N; ++c) W[p + (long long)c * ld] = czero<V>();
-        } else if (!pivoted && tid != pn) {
-            const double twx = tau * w.x, twy = tau * w.y;
-            double2 acc = make_double2(0.0, 0.0);
-            double nz = 0.0;
-            V* row = W + tid;
-            auto step = [&](const V xv, const int c) {
-                const double2 x = to_d2(xv);
-                const double2 q = ucur[c];
-                const V z = from_d2<V>(make_double2(x.x - (twx * q.x - twy * q.y), x.y - (twx * q.y + twy * q.x)));
-                row[(long long)c * ld] = z;
-                const double2 zd = to_d2(z);
-                const double2 un = unext[c];
-                acc.x += zd.x * un.x + zd.y * un.y;
-                acc.y += zd.y * un.x - zd.x * un.y;
-                nz += zd.x * zd.x + zd.y * zd.y;
-            };
-            // columns in chunks of LQ_U, the loads of the next chunk issued before the current one
-            // is applied and stored, so two chunks of memory latency overlap per thread
-            int c = k + 1;
-            const int nfull = (N - c) / LQ_U;
-            if (nfull > 0) {
-                V cur[LQ_U];
-#pragma unroll
-                for (int j = 0; j < LQ_U; ++j) cur[j] = row[(long long)(c + j) * ld];
-                for (int it = 0; it < nfull; ++it, c += LQ_U) {
-                    V nxt[LQ_U];
-                    if (it + 1 < nfull) {
-#pragma unroll
-                        for (int j = 0; j < LQ_U; ++j) nxt[j] = row[(long long)(c + LQ_U + j) * ld];
-                    }
-#pragma unroll
-                    for (int j = 0; j < LQ_U; ++j) step(cur[j], c + j);
-#pragma unroll
-                    for (int j = 0; j < LQ_U; ++j) cur[j] = nxt[j];
+    int k = 0;
+    while (k < kmax) {
+        int jn = 0;  // reflectors of this panel so far
+        for (; jn < LQ_B && k < kmax; ++jn, ++k) {
+            const int p = block_argmax(pivoted ? -1.0 : nrm, rv, ri);
+            // reflector from row p's current values, columns >= k
+            double2* u = U + jn * LQ_MAXN;
+            double part = 0.0;
+            for (int c = k + tid; c < N; c += blockDim.x) {
+                double2 x = to_d2(W[p + (long long)c * ld]);
+                for (int j = 0; j < jn; ++j) {
+                    const double2 t = cm(TW[j * LQ_NT + p], U[j * LQ_MAXN + c]);
+                    x.x -= t.x;
+                    x.y -= t.y;
+                }
+                u[c] = x;
+                part += x.x * x.x + x.y * x.y;
+            }
+            const double alpha2 = block_sum(part, rv);  // ends with a barrier: u complete
+            if (tid == 0) {
+                const double alpha = sqrt(alpha2);
+                const double2 x0 = u[k];
+                const double a0 = sqrt(x0.x * x0.x + x0.y * x0.y);
+                const double ex = a0 > 0.0 ? x0.x / a0 : 1.0, ey = a0 > 0.0 ? x0.y / a0 : 0.0;
+                if (alpha > 0.0) {
+                    s_d = make_double2(-ex * alpha, -ey * alpha);
+                    s_tau = 1.0 / (alpha * (alpha + a0));
+                    u[k] = make_double2(ex * (a0 + alpha), ey * (a0 + alpha));
+                } else {  // the rest of theta is zero: the identity
+                    s_d = make_double2(0.0, 0.0);
+                    s_tau = 0.0;
                 }
             }
-            for (; c < N; ++c) step(row[(long long)c * ld], c);
-            w = acc;
+            __syncthreads();
+            // g_j = u_j . conj(u) over columns >= k, for the panel's earlier reflectors
+            if (jn > 0) {
+                double gv[LQ_RED];
+                for (int q = 0; q < 2 * jn; ++q) gv[q] = 0.0;
+                for (int c = k + tid; c < N; c += blockDim.x) {
+                    const double2 uc = u[c];
+                    for (int j = 0; j < jn; ++j) {
+                        const double2 t = cmc(U[j * LQ_MAXN + c], uc);
+                        gv[2 * j] += t.x;
+                        gv[2 * j + 1] += t.y;
+                    }
+                }
+                block_sum_n(gv, 2 * jn, red, s_red);
+            }
+            const double tau = s_tau;
+            const double2 d = s_d;
+            // the pivot row takes its diagonal entry and zeros to its right; every other free row
+            // reads its trailing columns once: w = X[i, k:] . conj(u), corrected by the panel's
+            // pending updates (- sum_j tw_j[i] g_j), then its final column-k value
+            if (tid == p) {
+                W[p + (long long)k * ld] = from_d2<V>(d);
+                for (int c = k + 1; c < N; ++c) W[p + (long long)c * ld] = czero<V>();
+                pivoted = true;
+            } else if (!pivoted) {
+                double2 acc = make_double2(0.0, 0.0);
+                const double2 xk = to_d2(row[(long long)k * ld]);
+                {
+                    const double2 t = cmc(xk, u[k]);
+                    acc.x += t.x;
+                    acc.y += t.y;
+                }
+                int c = k + 1;
+                const int nfull = (N - c) / LQ_U;
+                if (nfull > 0) {
+                    V cur[LQ_U];
+#pragma unroll
+                    for (int j = 0; j < LQ_U; ++j) cur[j] = row[(long long)(c + j) * ld];
+                    for (int it = 0; it < nfull; ++it, c += LQ_U) {
+                        V nxt[LQ_U];
+                        if (it + 1 < nfull) {
+#pragma unroll
+                            for (int j = 0; j < LQ_U; ++j) nxt[j] = row[(long long)(c + LQ_U + j) * ld];
+                        }
+#pragma unroll
+                        for (int j = 0; j < LQ_U; ++j) {
+                            const double2 t = cmc(to_d2(cur[j]), u[c + j]);
+                            acc.x += t.x;
+                            acc.y += t.y;
+                            cur[j] = nxt[j];
+                        }
+                    }
+                }
+                for (; c < N; ++c) {
+                    const double2 t = cmc(to_d2(row[(long long)c * ld]), u[c]);
+                    acc.x += t.x;
+                    acc.y += t.y;
+                }
+                for (int j = 0; j < jn; ++j) {
+                    const double2 t = cm(TW[j * LQ_NT + tid], make_double2(s_red[2 * j], s_red[2 * j + 1]));
+                    acc.x -= t.x;
+                    acc.y -= t.y;
+                }
+                const double2 tw = make_double2(tau * acc.x, tau * acc.y);
+                TW[jn * LQ_NT + tid] = tw;
+                double2 col = xk;
+                for (int j = 0; j <= jn; ++j) {
+                    const double2 t = cm(TW[j * LQ_NT + tid], U[j * LQ_MAXN + k]);
+                    col.x -= t.x;
+                    col.y -= t.y;
+                }
+                const V cv = from_d2<V>(col);
+                row[(long long)k * ld] = cv;
+                const double2 cd = to_d2(cv);
+                nrm = fmax(0.0, nrm - (cd.x * cd.x + cd.y * cd.y));
+            }
+            __syncthreads();  // TW[jn] complete; s_red, s_tau, s_d free
+        }
+        // panel end: the panel's updates into columns >= k of every free row, exact norms
+        if (!pivoted && k < N) {
+            double2 tw[LQ_B];
+#pragma unroll
+            for (int j = 0; j < LQ_B; ++j) tw[j] = j < jn ? TW[j * LQ_NT + tid] : make_double2(0.0, 0.0);
+            double nz = 0.0;
+            for (int c = k; c < N; ++c) {
+                double2 x = to_d2(row[(long long)c * ld]);
+#pragma unroll
+                for (int j = 0; j < LQ_B; ++j) {
+                    if (j < jn) {
+                        const double2 t = cm(tw[j], U[j * LQ_MAXN + c]);
+                        x.x -= t.x;
+                        x.y -= t.y;
+                    }
+                }
+                const V z = from_d2<V>(x);
+                row[(long long)c * ld] = z;
+                const double2 zd = to_d2(z);
+                nz += zd.x * zd.x + zd.y * zd.y;
+            }
             nrm = nz;
         }
-        tau = s_tau;
-        d = s_d;
-        __syncthreads();  // the pass has read ucur and unext; s_tau, s_d, s_tw free
-        double2* t = ucur;
-        ucur = unext;
-        unext = t;
-        p = pn;
+        __syncthreads();  // the next panel rewrites U and TW
     }
-    __syncthreads();
 }
 
 template <typename T>
@@ -250,7 +292,7 @@ __global__ void __launch_bounds__(LQ_NT, 1) k_lq_batch(const InstTask<T>* insts,
     }
 }
 
-size_t lq_smem_bytes() { return sizeof(double2) * 2 * LQ_MAXN; }
+size_t lq_smem_bytes() { return sizeof(double2) * LQ_B * (LQ_MAXN + LQ_NT); }
 
 template <typename T>
 void launch_lq_batch(const InstTask<T>* insts, const UpdRef* refs, int nref, cudaStream_t s) {

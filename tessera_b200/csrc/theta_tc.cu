@@ -11,13 +11,15 @@
 //   D_re = A' B_re^T = Re(A C),  D_im = A' B_im^T = Im(A C).
 // A CTA owns 64 a x 64 b: M = 128 rows m = 2(a - a0) + s1, N = 128 columns n = 64 s2 + (b - b0);
 // D_re and D_im take 2 x 128 of the 512 tensor-memory columns.  K runs over mid in chunks of 16
-// complex (K' = 32 real = 4 MMAs of K = 8 per pass).  Operands are staged by the CTA's 128
+// complex (K' = 32 real = 4 MMAs of K = 8 per pass).  Operands are staged by the CTA's 256
 // threads into shared memory in the canonical K-major layout without swizzle (8-row x 16-byte
 // core matrices: rows 16 B apart, 8-row groups 128 B apart (SBO), 16-byte K chunks 2 KiB apart
-// (LBO)); one elected thread issues the MMAs and commits them to an mbarrier.  The gate
-// epilogue reads D row by row from tensor memory (warp w owns lanes 32w..32w+31), swaps the
-// s1 partner row with a lane shuffle, applies the 4x4 gate and writes theta and its Jacobi
-// copy W.  Rows, columns and K beyond the bond dimensions are zero-padded, so any bond works.
+// (LBO)), in two buffers: one elected thread issues a chunk's MMAs and commits them to that
+// buffer's mbarrier, and the threads go on to stage the next chunk into the other buffer while
+// the tensor cores work; a buffer is restaged only after its previous MMAs completed.  The gate
+// epilogue reads D row by row from tensor memory (warp w owns lanes 32 (w % 4) .. + 31; the two
+// warp groups take the two halves of the columns), swaps the s1 partner row with a lane
+// shuffle, applies the 4x4 gate and writes theta and its Jacobi copy W.  Rows, columns and K beyond the bond dimensions are zero-padded, so any bond works.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -42,11 +44,12 @@ constexpr int TC_KC = 16;    // complex K per chunk
 constexpr int TC_M = 2 * TC_BM;
 constexpr int TC_N = 2 * TC_BN;
 constexpr int TC_KR = 2 * TC_KC;            // real K per chunk
-constexpr int TC_NT = 128;
+constexpr int TC_NT = 256;                     // two warp groups: both stage, each reads half the columns
 constexpr int TC_OP_BYTES = TC_M * TC_KR * 4;  // one operand tile (128 rows x 32 floats) = 16 KiB
 constexpr int TC_LBO = (TC_M / 8) * 128;       // bytes between 16-byte K chunks
 constexpr int TC_SBO = 128;                    // bytes between 8-row groups
-constexpr int TC_SMEM = 6 * TC_OP_BYTES;       // A hi/lo, B_re hi/lo, B_im hi/lo
+constexpr int TC_STAGE = 6 * TC_OP_BYTES;      // one buffer: A hi/lo, B_re hi/lo, B_im hi/lo
+constexpr int TC_SMEM = 2 * TC_STAGE;          // two buffers: chunk k+1 is staged under chunk k's MMAs
 constexpr int TC_TMEM_COLS = 2 * TC_N;         // D_re, D_im
 
 static_assert(TC_M == 128 && TC_N % 16 == 0 && TC_N <= 256, "tcgen05 kind::tf32 shape");
@@ -121,7 +124,7 @@ __device__ __forceinline__ void tc_gate(const GateOp& op, const ScheduleView& sc
 __device__ void theta_tc_tile(const MpsView<float>& mps, const ScheduleView& sch, const GateOp& op,
                               const SvdWork<float>& wk, int tile_a, int tile_b, unsigned char* smem) {
     using V = float2;
-    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ __align__(8) uint64_t s_bar[2];  // MMAs of the chunk staged in buffer 0 / 1 done
     __shared__ uint32_t s_taddr;
     __shared__ int s_ok;
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -132,13 +135,10 @@ __device__ void theta_tc_tile(const MpsView<float>& mps, const ScheduleView& sch
     const int cap = mps.cap;
     const V* A = mps.site(i);
     const V* Cm = mps.site(i + 1);
-    unsigned char* opA_hi = smem;
-    unsigned char* opA_lo = smem + TC_OP_BYTES;
-    unsigned char* opR_hi = smem + 2 * TC_OP_BYTES;
-    unsigned char* opR_lo = smem + 3 * TC_OP_BYTES;
-    unsigned char* opI_hi = smem + 4 * TC_OP_BYTES;
-    unsigned char* opI_lo = smem + 5 * TC_OP_BYTES;
-    if (tid == 0) mbar_init(&s_bar, 1);
+    if (tid == 0) {
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+    }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_taddr)),
                      "r"(TC_TMEM_COLS)
@@ -150,38 +150,94 @@ __device__ void theta_tc_tile(const MpsView<float>& mps, const ScheduleView& sch
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_taddr;
     const uint32_t d_re = tmem, d_im = tmem + TC_N;
-    unsigned phase = 0;
+    unsigned phase = 0u;    // bit b: the parity to wait for on s_bar[b]
+    unsigned pending = 0u;  // bit b: a commit on buffer b not yet waited for
+    // one CTA-wide outcome per wait (thread 0 waits with a bound, the others re-check the phase)
+    auto wait_buf = [&](int b) -> bool {
+        const unsigned par = (phase >> b) & 1u;
+        if (tid == 0) s_ok = mbar_wait(&s_bar[b], par, 1000000000ull) ? 1 : 0;
+        __syncthreads();
+        const bool good = s_ok != 0;
+        if (good) {
+            if (tid != 0) mbar_wait(&s_bar[b], par, 1000000000ull);
+            phase ^= 1u << b;
+            pending &= ~(1u << b);
+        }
+        __syncthreads();  // s_ok free again
+        return good;
+    };
     bool ok = true;
     const int nchunk = (mid + TC_KC - 1) / TC_KC;
     for (int kc = 0; kc < nchunk && ok; ++kc) {
+        const int buf = kc & 1;
+        // the MMAs of chunk kc - 2 read this buffer: wait for them before restaging it
+        if (((pending >> buf) & 1u) && !wait_buf(buf)) { ok = false; break; }
+        unsigned char* opA_hi = smem + buf * TC_STAGE;
+        unsigned char* opA_lo = opA_hi + TC_OP_BYTES;
+        unsigned char* opR_hi = opA_hi + 2 * TC_OP_BYTES;
+        unsigned char* opR_lo = opA_hi + 3 * TC_OP_BYTES;
+        unsigned char* opI_hi = opA_hi + 4 * TC_OP_BYTES;
+        unsigned char* opI_lo = opA_hi + 5 * TC_OP_BYTES;
         const int c0 = kc * TC_KC;
-        // A' rows m = 2(a - a0) + s1 = site row 2 a0 + m: real parts at k' = kk, imaginary at TC_KC + kk
-        for (int e = tid; e < TC_M * TC_KC; e += TC_NT) {
-            const int m = e / TC_KC, kk = e - m * TC_KC;
-            const int a = a0 + (m >> 1), c = c0 + kk;
-            const V x = (a < dl && c < mid) ? A[(long long)(2 * a0 + m) * cap + c] : make_float2(0.f, 0.f);
-            const uint32_t hr = to_tf32(x.x), hi = to_tf32(x.y);
-            const uint32_t lr = to_tf32(x.x - __uint_as_float(hr)), li = to_tf32(x.y - __uint_as_float(hi));
-            *reinterpret_cast<uint32_t*>(opA_hi + tc_off(m, kk)) = hr;
-            *reinterpret_cast<uint32_t*>(opA_hi + tc_off(m, TC_KC + kk)) = hi;
-            *reinterpret_cast<uint32_t*>(opA_lo + tc_off(m, kk)) = lr;
-            *reinterpret_cast<uint32_t*>(opA_lo + tc_off(m, TC_KC + kk)) = li;
+        // Each task converts 4 consecutive k of one operand row and writes them as 16-byte
+        // vectors; a warp's 32 tasks are 32 consecutive rows (8-row groups of 128 contiguous
+        // bytes in the canonical layout), so the stores are free of bank conflicts.
+        // A' rows m = 2(a - a0) + s1 = site row 2 a0 + m: real parts at k' = k, imaginary at TC_KC + k.
+        // Lane l of a warp task takes row 8 task + (l & 7) and k = 4 (l >> 3) .. + 3: the four lanes
+        // of a row read its 128 contiguous bytes (two 16-byte loads each when the row pitch keeps
+        // them aligned), and lanes 0-7 of each store phase write eight different rows.
+        for (int t = tid; t < TC_M * (TC_KC / 4); t += TC_NT) {
+            const int lane = t & 31, m = 8 * (t >> 5) + (lane & 7), kq = lane >> 3;
+            const int a = a0 + (m >> 1), c = c0 + 4 * kq;
+            float2 xv[4];
+            const V* src = A + (long long)(2 * a0 + m) * cap + c;
+            if (a < dl && c + 3 < mid && (cap & 1) == 0) {
+                const float4 v0 = *reinterpret_cast<const float4*>(src);
+                const float4 v1 = *reinterpret_cast<const float4*>(src + 2);
+                xv[0] = make_float2(v0.x, v0.y); xv[1] = make_float2(v0.z, v0.w);
+                xv[2] = make_float2(v1.x, v1.y); xv[3] = make_float2(v1.z, v1.w);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) xv[j] = (a < dl && c + j < mid) ? src[j] : make_float2(0.f, 0.f);
+            }
+            uint4 hr, hi, lr, li;
+            uint32_t* phr = &hr.x; uint32_t* phi = &hi.x; uint32_t* plr = &lr.x; uint32_t* pli = &li.x;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                phr[j] = to_tf32(xv[j].x);
+                phi[j] = to_tf32(xv[j].y);
+                plr[j] = to_tf32(xv[j].x - __uint_as_float(phr[j]));
+                pli[j] = to_tf32(xv[j].y - __uint_as_float(phi[j]));
+            }
+            *reinterpret_cast<uint4*>(opA_hi + tc_off(m, 4 * kq)) = hr;
+            *reinterpret_cast<uint4*>(opA_hi + tc_off(m, TC_KC + 4 * kq)) = hi;
+            *reinterpret_cast<uint4*>(opA_lo + tc_off(m, 4 * kq)) = lr;
+            *reinterpret_cast<uint4*>(opA_lo + tc_off(m, TC_KC + 4 * kq)) = li;
         }
         // B rows n = TC_BN s2 + (b - b0): B_re = (Re C | -Im C), B_im = (Im C | Re C) along k'
-        for (int e = tid; e < TC_N * TC_KC; e += TC_NT) {
-            const int kk = e / TC_N, n = e - kk * TC_N;
-            const int s2 = n / TC_BN, b = b0 + (n - s2 * TC_BN), c = c0 + kk;
-            const V y = (b < dr && c < mid) ? Cm[(long long)(2 * c + s2) * cap + b] : make_float2(0.f, 0.f);
-            const uint32_t hr = to_tf32(y.x), hi = to_tf32(y.y);
-            const uint32_t lr = to_tf32(y.x - __uint_as_float(hr)), li = to_tf32(y.y - __uint_as_float(hi));
-            *reinterpret_cast<uint32_t*>(opR_hi + tc_off(n, kk)) = hr;
-            *reinterpret_cast<uint32_t*>(opR_hi + tc_off(n, TC_KC + kk)) = hi ^ 0x80000000u;
-            *reinterpret_cast<uint32_t*>(opR_lo + tc_off(n, kk)) = lr;
-            *reinterpret_cast<uint32_t*>(opR_lo + tc_off(n, TC_KC + kk)) = li ^ 0x80000000u;
-            *reinterpret_cast<uint32_t*>(opI_hi + tc_off(n, kk)) = hi;
-            *reinterpret_cast<uint32_t*>(opI_hi + tc_off(n, TC_KC + kk)) = hr;
-            *reinterpret_cast<uint32_t*>(opI_lo + tc_off(n, kk)) = li;
-            *reinterpret_cast<uint32_t*>(opI_lo + tc_off(n, TC_KC + kk)) = lr;
+        for (int t = tid; t < TC_N * (TC_KC / 4); t += TC_NT) {
+            const int n = t & (TC_N - 1), kq = t / TC_N;
+            const int s2 = n / TC_BN, b = b0 + (n - s2 * TC_BN), c = c0 + 4 * kq;
+            uint4 hr, hi, lr, li;
+            uint32_t* phr = &hr.x; uint32_t* phi = &hi.x; uint32_t* plr = &lr.x; uint32_t* pli = &li.x;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const V y = (b < dr && c + j < mid) ? Cm[(long long)(2 * (c + j) + s2) * cap + b] : make_float2(0.f, 0.f);
+                phr[j] = to_tf32(y.x);
+                phi[j] = to_tf32(y.y);
+                plr[j] = to_tf32(y.x - __uint_as_float(phr[j]));
+                pli[j] = to_tf32(y.y - __uint_as_float(phi[j]));
+            }
+            const uint4 nhi = make_uint4(hi.x ^ 0x80000000u, hi.y ^ 0x80000000u, hi.z ^ 0x80000000u, hi.w ^ 0x80000000u);
+            const uint4 nli = make_uint4(li.x ^ 0x80000000u, li.y ^ 0x80000000u, li.z ^ 0x80000000u, li.w ^ 0x80000000u);
+            *reinterpret_cast<uint4*>(opR_hi + tc_off(n, 4 * kq)) = hr;
+            *reinterpret_cast<uint4*>(opR_hi + tc_off(n, TC_KC + 4 * kq)) = nhi;
+            *reinterpret_cast<uint4*>(opR_lo + tc_off(n, 4 * kq)) = lr;
+            *reinterpret_cast<uint4*>(opR_lo + tc_off(n, TC_KC + 4 * kq)) = nli;
+            *reinterpret_cast<uint4*>(opI_hi + tc_off(n, 4 * kq)) = hi;
+            *reinterpret_cast<uint4*>(opI_hi + tc_off(n, TC_KC + 4 * kq)) = hr;
+            *reinterpret_cast<uint4*>(opI_lo + tc_off(n, 4 * kq)) = li;
+            *reinterpret_cast<uint4*>(opI_lo + tc_off(n, TC_KC + 4 * kq)) = lr;
         }
         // the tensor cores read shared memory through the async proxy
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -200,27 +256,26 @@ __device__ void theta_tc_tile(const MpsView<float>& mps, const ScheduleView& sch
                     tc_mma(d_re, da, tc_desc(sr[pb[p]] + koff), acc);
                     tc_mma(d_im, da, tc_desc(si[pb[p]] + koff), acc);
                 }
-            tc_commit(&s_bar);
+            tc_commit(&s_bar[buf]);
         }
-        // every thread waits for the MMAs (the operands are rewritten next chunk); one
-        // CTA-wide outcome
-        if (tid == 0) s_ok = mbar_wait(&s_bar, phase, 1000000000ull) ? 1 : 0;
-        __syncthreads();
-        ok = s_ok != 0;
-        if (ok) {
-            if (tid != 0) mbar_wait(&s_bar, phase, 1000000000ull);
-            phase ^= 1u;
-        }
+        pending |= 1u << buf;  // the next chunk stages the other buffer without waiting
+    }
+    // drain: the last commit covers every MMA issued before it; both barriers are consumed
+    for (int q = 0; q < 2 && ok; ++q) {
+        const int b = (nchunk - 2 + q) & 1;  // the older pending chunk first
+        if (((pending >> b) & 1u) && !wait_buf(b)) ok = false;
     }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (ok) {
         V g[16];
         tc_gate(op, sch, g);
-        // this thread's row m = tid (TMEM lane), a = a0 + m/2, s1 = m & 1
-        const int m = tid, s1 = m & 1, a = a0 + (m >> 1);
-        const uint32_t lane_off = (uint32_t)(32 * warp) << 16;
+        // row m (TMEM lane) of this thread: warp w reads lanes 32 (w % 4) .. + 31; the two warp
+        // groups take the two halves of the b columns
+        const int m = tid & (TC_M - 1), s1 = m & 1, a = a0 + (m >> 1);
+        const int half = tid / TC_M;
+        const uint32_t lane_off = (uint32_t)(32 * (warp & 3)) << 16;
         const int ld = wk.ld;
-        for (int j0 = 0; j0 < TC_BN; j0 += 16) {
+        for (int j0 = half * (TC_BN / 2); j0 < (half + 1) * (TC_BN / 2); j0 += 16) {
             float r0[16], i0[16], r1[16], i1[16];  // s2 = 0 and 1 columns
             tc_ld16(d_re + lane_off + j0, r0);
             tc_ld16(d_im + lane_off + j0, i0);
@@ -251,7 +306,8 @@ __device__ void theta_tc_tile(const MpsView<float>& mps, const ScheduleView& sch
         }
     } else if (tid == 0) {
         atomicOr(&wk.stats->status, ST_BARRIER_TIMEOUT);
-        mbar_wait(&s_bar, phase, 1000000000ull);  // let the MMAs in flight finish (bounded)
+        for (int b = 0; b < 2; ++b)  // let the MMAs in flight finish (bounded)
+            if ((pending >> b) & 1u) mbar_wait(&s_bar[b], (phase >> b) & 1u, 1000000000ull);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();

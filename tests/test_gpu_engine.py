@@ -424,7 +424,7 @@ def test_autotuner_times_every_candidate_and_picks_the_fastest():
     assert len(ch.measured) == len(autotune.candidates("c128"))
     times = {k: v["ms_per_update"] for k, v in ch.measured.items() if v["ms_per_update"] is not None}
     assert len(times) == len(ch.measured) and ch.ms_per_update == min(times.values())
-    assert (ch.jacobi_block, ch.theta_tensor_cores) in autotune.candidates("c128")
+    assert (ch.jacobi_block, ch.theta_tensor_cores, ch.jacobi_precondition) in autotune.candidates("c128")
 
 
 def test_mps_sampling_matches_state_probabilities():
