@@ -325,7 +325,7 @@ def plain_rate(args, local, peak_gbs=None, peak_tflops=None):
     from tessera_b200 import ffi
     p = workload(args, 0)
     s = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=args.chi, precision=args.precision,
-                    kernel_timing=True, device=local)
+                    kernel_timing=True, device=local, jacobi_precondition=1 if args.precondition == "on" else 2)
     s.randomize(1234)
     lo = 16 * min(32, args.n // 4)
     s.run_gates(MID_STEP, lo, lo + 2)
@@ -345,7 +345,10 @@ def plain_rate(args, local, peak_gbs=None, peak_tflops=None):
                 "hbm": {"achieved": gbs, "unit": "GB/s", "peak": peak_gbs,
                         "frac": gbs / peak_gbs if peak_gbs else None},
                 "compute": {"achieved": tfl, "unit": "TFLOP/s", "peak": peak_tflops,
-                            "frac": tfl / peak_tflops if peak_tflops else None}}
+                            "frac": tfl / peak_tflops if peak_tflops else None},
+                "precond_avg_launch_ms": (r.precond_ms - r0.precond_ms) / n,
+                "precond": "k_lq_coop (cooperative pivoted LQ, 8 rows of theta per CTA)"
+                           if args.precondition == "on" else "off"}
     return g / (r.device_ms / 1e3), r.device_ms / g, roof
 
 
@@ -522,7 +525,8 @@ def main():
     upd_per_step_inst = min(args.gates, p.updates_per_step())
     if B == 1:
         sess = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=args.chi, precision=args.precision,
-                           jacobi_block=args.jacobi_block, kernel_timing=True, device=local)
+                           jacobi_block=args.jacobi_block, kernel_timing=True, device=local,
+                           jacobi_precondition=1 if args.precondition == "on" else 2)
     else:
         sess = ffi.Session.batch(probs, chi=args.chi, precision=args.precision, jacobi_block=args.jacobi_block,
                                  kernel_timing=True, device=local, theta_tensor_cores=args.theta_tc,
@@ -749,7 +753,7 @@ def main():
     if rank == 0:
         cfg = config_dict(args, p)
         cfg.update({"jacobi_block": args.jacobi_block, "theta_tensor_cores": bool(args.theta_tc), "autotune": tuned,
-                    "jacobi_precondition": args.precondition if B > 1 else "off (cooperative single-instance SVD)"})
+                    "jacobi_precondition": args.precondition})
         cfg.update({"instances_per_gpu": B, "gates_per_step": G,
                     "step": f"{G} consecutive gate slots of the Trotter step at s=0.5 on each of {B} instances"})
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -362,9 +362,16 @@ public:
             svd_ms_ += ms;
         }
         timed_.clear();
+        for (auto& pr : timed_lq_) {
+            float ms = 0;
+            TQ_CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+            lq_ms_ += ms;
+        }
+        timed_lq_.clear();
         pool_next_ = 0;
         if (r) {
             r->svd_ms = svd_ms_;
+            r->precond_ms = lq_ms_;
             r->svd_bytes = st.svd_bytes;
             r->svd_flops = st.svd_flops;
             r->svd_launches = svd_launches_;
@@ -575,6 +582,7 @@ public:
         t.pp.max_sweeps = C_.max_sweeps;
         t.pp.rows_cap = rows_cap;
         t.pp.cols_cap = rows_cap;  // theta is at most 2 cap x 2 cap
+        t.pp.lq = 0;
         t.ent_steps = entc_;
         t.n_ent = n_ent_;
         t.pad = 0;
@@ -624,6 +632,8 @@ private:
     GateOp* res_ops_ = nullptr;
     int *res_off_ = nullptr, *res_order_ = nullptr, *res_work_ = nullptr;
     V *sites_ = nullptr, *theta_ = nullptr, *W_ = nullptr, *envs_ = nullptr, *xs_ = nullptr, *vbuf_ = nullptr;
+    void* lqc_ = nullptr;  // cooperative LQ candidate rows
+    bool lq_ok_ = false;
     int *dims_ = nullptr, *perm_ = nullptr, *counters_ = nullptr, *step_ = nullptr;
     double* scal_ = nullptr;
     double *sig2_ = nullptr, *sig_ = nullptr, *h_ = nullptr, *w_ = nullptr, *sa_ = nullptr, *sb_ = nullptr;
@@ -643,8 +653,8 @@ private:
     bool ran_ = false;
     double last_ms_ = 0.0;
     long long launches_ = 0, svd_launches_ = 0;
-    double svd_ms_ = 0.0;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timed_;
+    double svd_ms_ = 0.0, lq_ms_ = 0.0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timed_, timed_lq_;
     std::vector<cudaEvent_t> pool_;
     size_t pool_next_ = 0;
 
@@ -741,6 +751,9 @@ private:
         add((void**)&dotout_, sizeof(double) * (1 + n_ + m_));
         add((void**)&amp2_, sizeof(double));
         add((void**)&spins_d_, n_);
+        // candidate rows of the cooperative LQ (theta of 257..512 rows): 8 rows per CTA
+        lq_ok_ = ld_ > 256 && ld_ <= 512;
+        add((void**)&lqc_, lq_ok_ ? lq_coop_scratch_bytes(ld_, (int)es, (ld_ + 7) / 8) : 8);
         TQ_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         TQ_CK(device_alloc((void**)&base_, off));
         for (auto& it : plan) *it.second = base_ + it.first;
@@ -836,14 +849,32 @@ private:
             }
         }
         if (!tc_done) launch_theta<T>(M, sch, op, nullptr, work(), dl, dr, stream_);
+        // theta above 256 rows (the cooperative column-pair Jacobi): the pivoted LQ first, unless
+        // switched off or a block width was forced
+        const bool lq = lq_ok_ && C_.precond != 2 && C_.block == 0 && 2 * dl > 256 && 2 * dl <= 512 &&
+                        2 * dr <= 512;
         cudaEvent_t a = nullptr, b = nullptr;
+        if (lq) {
+            cudaEvent_t c = nullptr, d = nullptr;
+            if (C_.timing) {
+                c = event();
+                d = event();
+                TQ_CK(cudaEventRecord(c, stream_));
+            }
+            launch_lq_coop<T>(M, i, work(), lqc_, 2 * dl, 2 * dr, stream_);
+            if (C_.timing) {
+                TQ_CK(cudaEventRecord(d, stream_));
+                timed_lq_.push_back({c, d});
+            }
+            ++launches_;
+        }
         if (C_.timing) {
             a = event();
             b = event();
             TQ_CK(cudaEventRecord(a, stream_));
         }
         launch_svd<T>(M, i, C_.chi, tol_for(2 * dl), C_.max_sweeps, work(), 2 * dl, 2 * dr, pick_block(2 * dl, 2 * dr),
-                      stream_);
+                      stream_, 0, 0, lq ? 1 : 0);
         if (C_.timing) {
             TQ_CK(cudaEventRecord(b, stream_));
             timed_.push_back({a, b});

@@ -86,6 +86,8 @@ struct SvdParams {
     int max_sweeps;
     int rows_cap;      // shared-memory column length
     int cols_cap;      // shared-memory column count of the resident Jacobi (>= N, even)
+    int lq;            // 1: W holds the pivoted LQ factor P L of theta (lq.cu): the Jacobi takes
+                       //    min(R, N) columns (the rest are zero)
 };
 
 struct ChainStep {
@@ -125,7 +127,13 @@ void launch_theta(const MpsView<T>& mps, const ScheduleView& sch, GateOp op, con
 // R, N > 0 run a standalone SVD of an explicit R x N matrix in wk.W (no truncation).
 template <typename T>
 int launch_svd(const MpsView<T>& mps, int bond, int chi, double tol, int max_sweeps, SvdWork<T> wk,
-               int rows_ub, int cols_ub, int block_w, cudaStream_t s, int R = 0, int N = 0);
+               int rows_ub, int cols_ub, int block_w, cudaStream_t s, int R = 0, int N = 0, int lq = 0);
+// cooperative row-pivoted LQ of one theta's working copy, in place (lq.cu); rows_ub <= 1024
+// (the engine uses it for 257..512 rows)
+template <typename T>
+void launch_lq_coop(const MpsView<T>& mps, int bond, SvdWork<T> wk, void* scratch, int rows_ub, int cols_ub,
+                    cudaStream_t s);
+size_t lq_coop_scratch_bytes(int ld, int esz, int ctas);
 template <typename T>
 void launch_absorb(const MpsView<T>& mps, int bond, SvdWork<T> wk, int rows_ub, int cols_ub, int keep_ub,
                    cudaStream_t s);

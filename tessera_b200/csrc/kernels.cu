@@ -563,7 +563,8 @@ __device__ __forceinline__ void svd_body(const MpsView<T>& mps, const SvdWork<T>
     __syncthreads();
     const int tid = threadIdx.x;
     const int R = pp.R > 0 ? pp.R : 2 * mps.dims[pp.bond];
-    const int N = pp.N > 0 ? pp.N : 2 * mps.dims[pp.bond + 2];
+    const int N0 = pp.N > 0 ? pp.N : 2 * mps.dims[pp.bond + 2];
+    const int N = pp.lq && N0 > R ? R : N0;
     const int ld = wk.ld;
     V* W = wk.W;
     const int nb = (N + BW - 1) / BW;
@@ -950,7 +951,8 @@ __device__ void svd_resident_body(const MpsView<T>& mps, const SvdWork<T>& wk, c
     __shared__ double red[4 * 32];
     __shared__ int s_rot[2];
     const int R = pp.R > 0 ? pp.R : 2 * mps.dims[pp.bond];
-    const int N = pp.N > 0 ? pp.N : 2 * mps.dims[pp.bond + 2];
+    const int N0 = pp.N > 0 ? pp.N : 2 * mps.dims[pp.bond + 2];
+    const int N = pp.lq && N0 > R ? R : N0;
     const int rc = pp.rows_cap;
     V* col = reinterpret_cast<V*>(smraw);  // [cols_cap][rows_cap]
     if (R > rc || R > LPP * RES_RPL || N > pp.cols_cap) {  // host sizing bug guard
@@ -1672,7 +1674,8 @@ __device__ void svd_body_rc(const MpsView<T>& mps, const SvdWork<T>& wk, const S
     __shared__ int s_fail;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int R = pp.R > 0 ? pp.R : 2 * mps.dims[pp.bond];
-    const int N = pp.N > 0 ? pp.N : 2 * mps.dims[pp.bond + 2];
+    const int N0 = pp.N > 0 ? pp.N : 2 * mps.dims[pp.bond + 2];
+    const int N = pp.lq && N0 > R ? R : N0;
     const int rc = pp.rows_cap;
     const int ld = wk.ld;
     V* W = wk.W;
@@ -1952,11 +1955,7 @@ __global__ void __launch_bounds__(SvdShape<BW, RPL>::NT, 1) k_svd_batch(const In
         const InstTask<T>& it = insts[rf.inst];
         SvdParams pp = it.pp;
         pp.bond = rf.op.bond;
-        if (lq && pp.R <= 0) {
-            pp.R = 2 * it.mps.dims[pp.bond];
-            const int n = 2 * it.mps.dims[pp.bond + 2];
-            pp.N = n < pp.R ? n : pp.R;
-        }
+        pp.lq = lq;
         if constexpr (RPL > 0) svd_body_rc<T, BW, RPL>(it.mps, it.wk, pp, smraw);
         else svd_body<T, BW, RPL>(it.mps, it.wk, pp, 0, 1, smraw);
         __syncthreads();
@@ -1990,8 +1989,9 @@ static int svd_launch_bw(const MpsView<T>& mps, const SvdParams& pp, SvdWork<T> 
 
 template <typename T>
 int launch_svd(const MpsView<T>& mps, int bond, int chi, double tol, int max_sweeps, SvdWork<T> wk,
-               int rows_ub, int cols_ub, int block_w, cudaStream_t s, int R, int N) {
-    SvdParams pp;
+               int rows_ub, int cols_ub, int block_w, cudaStream_t s, int R, int N, int lq) {
+    SvdParams pp{};
+    pp.lq = lq;
     pp.bond = bond;
     pp.R = R;
     pp.N = N;
@@ -2637,7 +2637,7 @@ void launch_entropy_batch(const InstTask<T>* insts, int ninst, cudaStream_t s) {
     template void launch_theta<T>(const MpsView<T>&, const ScheduleView&, GateOp, const double*, SvdWork<T>, \
                                   int, int, cudaStream_t);                                                  \
     template int launch_svd<T>(const MpsView<T>&, int, int, double, int, SvdWork<T>, int, int, int,         \
-                               cudaStream_t, int, int);                                                     \
+                               cudaStream_t, int, int, int);                                                \
     template void launch_absorb<T>(const MpsView<T>&, int, SvdWork<T>, int, int, int, cudaStream_t);        \
     template void launch_chain<T>(const MpsView<T>&, int, const ChainStep*, int, cplx_t<T>*, cplx_t<T>*,   \
                                   GridBar*, RunStats*, int, cudaStream_t);                                  \

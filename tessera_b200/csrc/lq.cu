@@ -315,4 +315,200 @@ void launch_lq_batch(const InstTask<T>* insts, const UpdRef* refs, int nref, cud
 template void launch_lq_batch<double>(const InstTask<double>*, const UpdRef*, int, cudaStream_t);
 template void launch_lq_batch<float>(const InstTask<float>*, const UpdRef*, int, cudaStream_t);
 
+// ------------------------------------------------------------------------------------
+// The same LQ for the single-instance engine, cooperative over ceil(R / LQC_RB) CTAs: CTA g keeps
+// rows [g LQC_RB, (g + 1) LQC_RB) of W in shared memory for the whole factorization.  Per step
+// every CTA publishes its best unpivoted row (largest remaining norm) and that row's columns >= k
+// to a global candidate slot, one bounded grid barrier follows, and every CTA then picks the same
+// winner (largest norm, lowest row on ties), forms the reflector from the winner's row, and
+// updates its own rows in shared memory (exact norms recomputed).  The candidate slots alternate
+// between two buffers by step parity: a CTA rewrites the buffer of step k only after the barrier
+// of step k + 1, which every CTA passes after it has read step k's.  W is written back at the
+// end; if a barrier gives up, W keeps theta (the Jacobi then runs unpreconditioned) and the
+// status reports the timeout.
+// ------------------------------------------------------------------------------------
+constexpr int LQC_RB = 8;    // rows per CTA (2 LQC_RB <= LQ_RED values per reduction)
+constexpr int LQC_NT = 256;  // threads per CTA
+
+template <typename T>
+__global__ void __launch_bounds__(LQC_NT, 1) k_lq_coop(MpsView<T> mps, int bond, SvdWork<T> wk, cplx_t<T>* cand,
+                                                       double* keys, int* idxs) {
+    using V = cplx_t<T>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ double rv[LQC_NT / 32];
+    __shared__ double red[LQC_NT / 32][LQ_RED];
+    __shared__ double s_red[LQ_RED];
+    __shared__ double nrm[LQC_RB];
+    __shared__ int piv[LQC_RB];
+    __shared__ double s_tau;
+    __shared__ double2 s_d;
+    __shared__ int s_p, s_gc;
+    const int tid = threadIdx.x, cta = blockIdx.x, G = gridDim.x;
+    const int R = 2 * mps.dims[bond], N = 2 * mps.dims[bond + 2];
+    const int ld = wk.ld;
+    int* status = &wk.stats->status;
+    if (R > G * LQC_RB || N > LQ_MAXN) {  // host sizing bug guard (uniform over the grid)
+        if (cta == 0 && tid == 0) atomicOr(status, ST_BAD_DIMS);
+        return;
+    }
+    V* X = reinterpret_cast<V*>(smraw);               // [LQC_RB][N] this CTA's rows
+    double2* u = reinterpret_cast<double2*>(X + LQC_RB * N);  // [N] the step's reflector
+    const int r0 = cta * LQC_RB;
+    const int nr = R - r0 < LQC_RB ? (R - r0 > 0 ? R - r0 : 0) : LQC_RB;
+    for (int e = tid; e < LQC_RB * N; e += LQC_NT) {
+        const int r = e % LQC_RB, c = e / LQC_RB;  // 8 consecutive rows of a column: 128 contiguous bytes
+        X[r * N + c] = r < nr ? wk.W[(r0 + r) + (long long)c * ld] : czero<V>();
+    }
+    if (tid < LQC_RB) piv[tid] = tid < nr ? 0 : 1;
+    __syncthreads();
+    // exact row norms
+    {
+        double v[LQ_RED];
+        for (int r = 0; r < LQC_RB; ++r) v[r] = 0.0;
+        for (int c = tid; c < N; c += LQC_NT)
+            for (int r = 0; r < LQC_RB; ++r) {
+                const double2 x = to_d2(X[r * N + c]);
+                v[r] += x.x * x.x + x.y * x.y;
+            }
+        block_sum_n(v, LQC_RB, red, s_red);
+        if (tid < LQC_RB) nrm[tid] = s_red[tid];
+        __syncthreads();
+    }
+    const int kmax = R < N ? R : N;
+    for (int k = 0; k < kmax; ++k) {
+        const int par = k & 1;
+        // this CTA's candidate: its unpivoted row of largest remaining norm
+        if (tid == 0) {
+            double best = -1.0;
+            int br = -1;
+            for (int r = 0; r < nr; ++r)
+                if (!piv[r] && nrm[r] > best) { best = nrm[r]; br = r; }
+            keys[par * G + cta] = best;
+            idxs[par * G + cta] = br < 0 ? -1 : r0 + br;
+            s_p = br;
+        }
+        __syncthreads();
+        if (s_p >= 0)
+            for (int c = k + tid; c < N; c += LQC_NT) cand[((long long)par * G + cta) * ld + c] = X[s_p * N + c];
+        if (!grid_sync(wk.bar, status, (unsigned)G)) return;  // W untouched: still theta
+        // the winner, the same on every CTA
+        if (tid == 0) {
+            double best = -2.0;
+            int gc = -1, gr = 1 << 30;
+            for (int g = 0; g < G; ++g) {
+                const double kv = *(volatile double*)&keys[par * G + g];
+                const int rr = *(volatile int*)&idxs[par * G + g];
+                if (rr >= 0 && (kv > best || (kv == best && rr < gr))) { best = kv; gc = g; gr = rr; }
+            }
+            s_gc = gc;
+            s_p = gr;
+        }
+        __syncthreads();
+        const int gc = s_gc, p = s_p;
+        // reflector from the winner's row (published by its owner), columns >= k
+        double part = 0.0;
+        for (int c = k + tid; c < N; c += LQC_NT) {
+            const V* src = cand + ((long long)par * G + gc) * ld + c;
+            const double2 x = to_d2(*(const volatile V*)src);
+            u[c] = x;
+            part += x.x * x.x + x.y * x.y;
+        }
+        const double alpha2 = block_sum(part, rv);
+        if (tid == 0) {
+            const double alpha = sqrt(alpha2);
+            const double2 x0 = u[k];
+            const double a0 = sqrt(x0.x * x0.x + x0.y * x0.y);
+            const double ex = a0 > 0.0 ? x0.x / a0 : 1.0, ey = a0 > 0.0 ? x0.y / a0 : 0.0;
+            if (alpha > 0.0) {
+                s_d = make_double2(-ex * alpha, -ey * alpha);
+                s_tau = 1.0 / (alpha * (alpha + a0));
+                u[k] = make_double2(ex * (a0 + alpha), ey * (a0 + alpha));
+            } else {
+                s_d = make_double2(0.0, 0.0);
+                s_tau = 0.0;
+            }
+            if (p >= r0 && p < r0 + nr) piv[p - r0] = 1;
+        }
+        __syncthreads();
+        const double tau = s_tau;
+        const double2 d = s_d;
+        const int mine_p = (p >= r0 && p < r0 + nr) ? p - r0 : -1;
+        // products w_r = X[r, k:] . conj(u) of this CTA's unpivoted rows
+        double v[LQ_RED];
+        for (int q = 0; q < 2 * LQC_RB; ++q) v[q] = 0.0;
+        for (int c = k + tid; c < N; c += LQC_NT) {
+            const double2 uc = u[c];
+            for (int r = 0; r < LQC_RB; ++r) {
+                const double2 t = cmc(to_d2(X[r * N + c]), uc);
+                v[2 * r] += t.x;
+                v[2 * r + 1] += t.y;
+            }
+        }
+        block_sum_n(v, 2 * LQC_RB, red, s_red);
+        double2 tw[LQC_RB];
+        bool upd[LQC_RB];
+        for (int r = 0; r < LQC_RB; ++r) {
+            upd[r] = r < nr && !piv[r];
+            tw[r] = make_double2(tau * s_red[2 * r], tau * s_red[2 * r + 1]);
+        }
+        __syncthreads();  // s_red read by every thread before the norm sums reuse it
+        // updates and exact remaining norms; the pivot row takes d and zeros to its right
+        for (int q = 0; q < LQC_RB; ++q) v[q] = 0.0;
+        for (int c = k + tid; c < N; c += LQC_NT) {
+            const double2 uc = u[c];
+            for (int r = 0; r < LQC_RB; ++r) {
+                if (r == mine_p) {
+                    X[r * N + c] = c == k ? from_d2<V>(d) : czero<V>();
+                } else if (upd[r]) {
+                    const double2 x = to_d2(X[r * N + c]);
+                    const double2 t = cm(tw[r], uc);
+                    const V z = from_d2<V>(make_double2(x.x - t.x, x.y - t.y));
+                    X[r * N + c] = z;
+                    if (c > k) {
+                        const double2 zd = to_d2(z);
+                        v[r] += zd.x * zd.x + zd.y * zd.y;
+                    }
+                }
+            }
+        }
+        block_sum_n(v, LQC_RB, red, s_red);
+        if (tid < LQC_RB && tid < nr && !piv[tid]) nrm[tid] = s_red[tid];
+        __syncthreads();
+    }
+    // this CTA's rows of P L back to W
+    for (int e = tid; e < LQC_RB * N; e += LQC_NT) {
+        const int r = e % LQC_RB, c = e / LQC_RB;
+        if (r < nr) wk.W[(r0 + r) + (long long)c * ld] = X[r * N + c];
+    }
+}
+
+size_t lq_coop_smem_bytes(int N, int esz) { return (size_t)LQC_RB * N * esz + sizeof(double2) * N; }
+
+// Candidate buffer of the cooperative LQ: two parities of up to `ctas` rows of `ld` elements, plus
+// keys and row indices.
+size_t lq_coop_scratch_bytes(int ld, int esz, int ctas) {
+    return (size_t)2 * ctas * ld * esz + (size_t)2 * ctas * (sizeof(double) + sizeof(int)) + 64;
+}
+
+template <typename T>
+void launch_lq_coop(const MpsView<T>& mps, int bond, SvdWork<T> wk, void* scratch, int rows_ub, int cols_ub,
+                    cudaStream_t s) {
+    using V = cplx_t<T>;
+    const int G = (rows_ub + LQC_RB - 1) / LQC_RB;
+    V* cand = reinterpret_cast<V*>(scratch);
+    double* keys = reinterpret_cast<double*>(cand + (size_t)2 * G * wk.ld);
+    int* idxs = reinterpret_cast<int*>(keys + 2 * G);
+    const size_t smem = lq_coop_smem_bytes(cols_ub, (int)sizeof(V));
+    auto fn = k_lq_coop<T>;
+    TQ_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    MpsView<T> m = mps;
+    int b = bond;
+    void* args[] = {&m, &b, &wk, &cand, &keys, &idxs};
+    TQ_CHECK(cudaLaunchCooperativeKernel((const void*)fn, dim3(G), dim3(LQC_NT), args, smem, s));
+}
+
+template void launch_lq_coop<double>(const MpsView<double>&, int, SvdWork<double>, void*, int, int, cudaStream_t);
+template void launch_lq_coop<float>(const MpsView<float>&, int, SvdWork<float>, void*, int, int, cudaStream_t);
+
+
 }  // namespace tq

@@ -143,8 +143,8 @@ def problem_struct(h, ei, ej, ew, sa, sb, bias=None, sc=None):
 def config_struct(dt=0.1, chi=32, precision="c128", zz_substeps=1, jacobi_tol=0.0, jacobi_max_sweeps=0,
                   jacobi_block=0, device=-1, step_begin=0, step_end=0, initial_mps=None, skip_observables=False,
                   theta_tensor_cores=False, jacobi_precondition=0):
-    """jacobi_precondition: 0 default (on), 1 on, 2 off -- the pivoted LQ before the batched
-    column-pair Jacobi of theta above 256 rows."""
+    """jacobi_precondition: 0 default (on), 1 on, 2 off -- the pivoted LQ before the column-pair
+    Jacobi of theta above 256 rows (batched: one CTA per theta; single instance: cooperative)."""
     L = _lib.load()
     c = _lib.Config()
     L.tessera_qa_config_init(C.byref(c))

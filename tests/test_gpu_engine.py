@@ -592,11 +592,11 @@ def chi256_window(oracle):
     return p, step, q0, start, o_sites, st
 
 
-@pytest.mark.parametrize("batched", [False, "lq", "plain"])
-def test_truncating_chi256_updates_match_the_oracle(chi256_window, batched):
+@pytest.mark.parametrize("batched,precond", [(False, 1), (False, 2), (True, 1), (True, 2)])
+def test_truncating_chi256_updates_match_the_oracle(chi256_window, batched, precond):
     """Three truncating chi=256 updates (512 x 512 theta) through the cooperative single-instance
-    SVD and the batched block-row-cyclic SVD, the latter with ("lq") and without ("plain") the
-    pivoted-LQ preconditioner, against the oracle.  The cut is well conditioned
+    SVD and the batched block-row-cyclic SVD, each with (1) and without (2) the pivoted-LQ
+    preconditioner (cooperative or one CTA per theta), against the oracle.  The cut is well conditioned
     (relative gap at the cut above 1e-4 in every update), so two accurate SVDs differ there by
     rounding over the gap: the states agree to infidelity 1e-12, the discarded-weight ratio to
     1e-6 relative, and the kept singular values (left-slice norms of the sites last written as
@@ -604,9 +604,9 @@ def test_truncating_chi256_updates_match_the_oracle(chi256_window, batched):
     p, step, q0, start, o_sites, st = chi256_window
     assert st["updates"] == 3 and st["min_cut_gap"] > 1e-4 and st["max_trunc"] > 1e-3
     if batched:
-        s = ffi.Session.batch([p], chi=256, jacobi_precondition=1 if batched == "lq" else 2)
+        s = ffi.Session.batch([p], chi=256, jacobi_precondition=precond)
     else:
-        s = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=256)
+        s = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=256, jacobi_precondition=precond)
     s.randomize(31)
     s.run_gates(step, q0, q0 + 3)
     r = s.sync()
@@ -620,6 +620,42 @@ def test_truncating_chi256_updates_match_the_oracle(chi256_window, batched):
     for i, (g, o) in enumerate(zip(g_sites, o_sites)):
         ng, no = left_norms(g), left_norms(o)
         assert np.max(np.abs(ng - no) / no) < 1e-10, i
+
+
+@pytest.mark.parametrize("precond", [1, 2])
+def test_graded_chi256_updates_match_the_oracle(oracle, precond):
+    """The bench's second input: a random MPS whose site columns fall off as exp(-b/24), so
+    each theta's spectrum is graded like a TEBD state's Schmidt values (tessera_qa_session_
+    randomize_graded).  Three chi=256 updates (512 x 512 theta) through the batched Jacobi with
+    and without the pivoted-LQ preconditioner, against the oracle on the same start: infidelity
+    under 1e-12, the (tiny) discarded weights equal to 1e-12 absolute, the left-slice norms of
+    every site within 1e-10 relative where they exceed 1e-3 of the site's largest and within
+    1e-12 of it elsewhere (the graded tail reaches the rounding floor)."""
+    p = instances.chain_range(n=40, dmax=4, seed=2, T=50.0, dt=0.02, chi=256)
+    step = len(p.sa) // 2
+    bonds = []
+    for i, j in zip(p.ei, p.ej):
+        bonds += [k - 1 for k in range(int(j), int(i) + 1, -1)] + [int(i)] + [k for k in range(int(i) + 1, int(j))]
+    q0 = next(q for q, b in enumerate(bonds) if b >= 16)
+    s = ffi.Session.batch([p], chi=256, jacobi_precondition=precond)
+    s.randomize(31, decay=24.0)
+    start = ffi.checkpoint_to_sites(s.save_instance(0))[1]
+    s.run_gates(step, q0, q0 + 3)
+    r = s.sync()
+    ck = s.save_instance(0)
+    s.close()
+    assert r.status == 0 and r.two_site_updates == 3
+    inst = Instance(p.h, p.ei.astype(np.int32), p.ej.astype(np.int32), p.ew)
+    o_sites, st = oracle.apply_slots(inst, start, float(p.sb[step]), p.dt, 256, q0, q0 + 3)
+    g_sites = ffi.checkpoint_to_sites(ck)[1]
+    assert [t.shape for t in g_sites] == [t.shape for t in o_sites]
+    assert 1 - mps_fidelity(g_sites, o_sites) < 1e-12
+    assert abs(r.max_trunc - st["max_trunc"]) < 1e-12
+    for i, (g, o) in enumerate(zip(g_sites, o_sites)):
+        ng, no = left_norms(g), left_norms(o)
+        big = no > 1e-3 * no.max()
+        assert np.max(np.abs(ng[big] - no[big]) / no[big]) < 1e-10, i
+        assert np.max(np.abs(ng - no)) < 1e-12 * no.max(), i
 
 
 def test_graph_captured_steps_equal_launched_steps():
