@@ -336,18 +336,19 @@ __global__ void __launch_bounds__(LQC_NT, 1) k_lq_coop(MpsView<T> mps, int bond,
     using V = cplx_t<T>;
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ double rv[LQC_NT / 32];
+    __shared__ int ri[LQC_NT / 32];
     __shared__ double red[LQC_NT / 32][LQ_RED];
     __shared__ double s_red[LQ_RED];
     __shared__ double nrm[LQC_RB];
     __shared__ int piv[LQC_RB];
-    __shared__ double s_tau;
+    __shared__ double s_tau, s_a2;
     __shared__ double2 s_d;
     __shared__ int s_p, s_gc;
     const int tid = threadIdx.x, cta = blockIdx.x, G = gridDim.x;
     const int R = 2 * mps.dims[bond], N = 2 * mps.dims[bond + 2];
     const int ld = wk.ld;
     int* status = &wk.stats->status;
-    if (R > G * LQC_RB || N > LQ_MAXN) {  // host sizing bug guard (uniform over the grid)
+    if (R > G * LQC_RB || N > LQ_MAXN || G > LQC_NT) {  // host sizing bug guard (uniform over the grid)
         if (cta == 0 && tid == 0) atomicOr(status, ST_BAD_DIMS);
         return;
     }
@@ -391,31 +392,31 @@ __global__ void __launch_bounds__(LQC_NT, 1) k_lq_coop(MpsView<T> mps, int bond,
         if (s_p >= 0)
             for (int c = k + tid; c < N; c += LQC_NT) cand[((long long)par * G + cta) * ld + c] = X[s_p * N + c];
         if (!grid_sync(wk.bar, status, (unsigned)G)) return;  // W untouched: still theta
-        // the winner, the same on every CTA
-        if (tid == 0) {
-            double best = -2.0;
-            int gc = -1, gr = 1 << 30;
-            for (int g = 0; g < G; ++g) {
-                const double kv = *(volatile double*)&keys[par * G + g];
-                const int rr = *(volatile int*)&idxs[par * G + g];
-                if (rr >= 0 && (kv > best || (kv == best && rr < gr))) { best = kv; gc = g; gr = rr; }
-            }
-            s_gc = gc;
-            s_p = gr;
+        // the winner, the same on every CTA: thread g reads CTA g's candidate, then a block argmax
+        // (largest norm; ties to the lowest CTA, which holds the lowest row)
+        double kv = -2.0;
+        int rr = -1;
+        if (tid < G) {
+            kv = *(volatile double*)&keys[par * G + tid];
+            rr = *(volatile int*)&idxs[par * G + tid];
+            if (rr < 0) kv = -2.0;
+        }
+        const int gw = block_argmax(kv, rv, ri);
+        if (tid == gw) {
+            s_gc = gw;
+            s_p = rr;
+            s_a2 = kv;  // the winner's exact remaining norm^2 (summed from the stored values)
         }
         __syncthreads();
         const int gc = s_gc, p = s_p;
         // reflector from the winner's row (published by its owner), columns >= k
-        double part = 0.0;
         for (int c = k + tid; c < N; c += LQC_NT) {
             const V* src = cand + ((long long)par * G + gc) * ld + c;
-            const double2 x = to_d2(*(const volatile V*)src);
-            u[c] = x;
-            part += x.x * x.x + x.y * x.y;
+            u[c] = to_d2(*(const volatile V*)src);
         }
-        const double alpha2 = block_sum(part, rv);
+        __syncthreads();
         if (tid == 0) {
-            const double alpha = sqrt(alpha2);
+            const double alpha = sqrt(fmax(s_a2, 0.0));
             const double2 x0 = u[k];
             const double a0 = sqrt(x0.x * x0.x + x0.y * x0.y);
             const double ex = a0 > 0.0 ? x0.x / a0 : 1.0, ey = a0 > 0.0 ? x0.y / a0 : 0.0;
