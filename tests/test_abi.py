@@ -50,7 +50,7 @@ def test_bad_schedule_rejected_like_rust():
     assert e.value.err is ffi.QaError.BadSchedule
 
 
-@pytest.mark.parametrize("case", ["nan_h", "edge_oob", "chi0", "n0", "nan_sched", "bad_dt", "bad_block"])
+@pytest.mark.parametrize("case", ["nan_h", "edge_oob", "chi0", "n0", "nan_sched", "bad_dt", "bad_block", "bad_precond"])
 def test_invalid_input_returns_einval_without_a_gpu(case):
     h = np.array([0.1, -0.2, 0.3])
     ei, ej, ew = np.array([0, 1]), np.array([1, 2]), np.array([0.5, -0.5])
@@ -71,6 +71,8 @@ def test_invalid_input_returns_einval_without_a_gpu(case):
         kw["dt"] = -1.0
     elif case == "bad_block":
         kw["jacobi_block"] = 3
+    elif case == "bad_precond":
+        kw["jacobi_precondition"] = 3
     with pytest.raises(_lib.EngineError) as e:
         ffi.anneal(h, ei, ej, ew, sa, sb, **kw)
     assert e.value.code == _lib.EINVAL
