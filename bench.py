@@ -594,7 +594,8 @@ def main():
         try:
             with open(tf) as f:
                 d = json.load(f)
-            if d.get("chi") == args.chi and d.get("precision") == args.precision and d.get("batch") == B:
+            if (d.get("chi") == args.chi and d.get("precision") == args.precision and d.get("batch") == B
+                    and d.get("jacobi_precondition", "off") == args.precondition):
                 traffic = d.get("dram_bytes_per_launch")
         except Exception:
             traffic = None
