@@ -113,6 +113,57 @@ def pivoted_lq(A: np.ndarray) -> np.ndarray:
     return X
 
 
+def pivoted_lq_blocked(A: np.ndarray, panel: int = 8) -> np.ndarray:
+    """pivoted_lq with the updates delayed over panels, as lq.cu's k_lq_batch runs it: within a
+    panel the trailing block is not updated; row i's current values are X[i, c] - sum_j tw_j[i]
+    u_j[c] over the panel's reflectors (tw_j = tau_j w_j), each step's products X[i, k:] . conj(u)
+    are corrected by g_j = u_j . conj(u), only column k is written per step, and the panel's
+    updates are applied at its end, where the row norms are recomputed exactly."""
+    X = np.array(A, dtype=np.complex128, copy=True)
+    R, N = X.shape
+    kmax = min(R, N)
+    free = np.ones(R, bool)
+    nrm = np.sum(np.abs(X) ** 2, axis=1)
+    k = 0
+    while k < kmax:
+        us, tws = [], []
+        while k < kmax and len(us) < panel:
+            key = np.where(free, nrm, -1.0)
+            p = int(np.flatnonzero(key == key.max())[0])
+            x = X[p, k:].copy()
+            for u, tw in zip(us, tws):
+                x -= tw[p] * u[k:]
+            alpha, a0 = np.sqrt(np.sum(np.abs(x) ** 2)), abs(x[0])
+            e = x[0] / a0 if a0 > 0 else 1.0
+            u = np.zeros(N, complex)
+            u[k:] = x
+            tau = 0.0
+            if alpha > 0:
+                u[k] = e * (a0 + alpha)
+                tau = 1.0 / (alpha * (alpha + a0))
+            free[p] = False
+            X[p, k] = -e * alpha if alpha > 0 else 0
+            X[p, k + 1:] = 0
+            rows = np.flatnonzero(free)
+            w = np.zeros(R, complex)
+            w[rows] = X[rows, k:] @ np.conj(u[k:])
+            for uj, tj in zip(us, tws):
+                w[rows] -= tj[rows] * np.sum(uj[k:] * np.conj(u[k:]))
+            us.append(u)
+            tws.append(tau * w)
+            col = X[rows, k].copy()
+            for uj, tj in zip(us, tws):
+                col -= tj[rows] * uj[k]
+            X[rows, k] = col
+            nrm[rows] = np.maximum(0.0, nrm[rows] - np.abs(col) ** 2)
+            k += 1
+        rows = np.flatnonzero(free)
+        for uj, tj in zip(us, tws):
+            X[np.ix_(rows, np.arange(k, N))] -= np.outer(tj[rows], uj[k:])
+        nrm[rows] = np.sum(np.abs(X[rows, k:]) ** 2, axis=1)
+    return X
+
+
 def graded(n: int, decay: float, seed: int) -> tuple[np.ndarray, np.ndarray]:
     """n x n matrix U diag(exp(-k/decay)) V^H with Haar-like random unitary U, V."""
     rng = np.random.Generator(np.random.PCG64(seed))

@@ -8,7 +8,7 @@ sweep still rotates >= 10% of its pairs, then rule A) resolves them at the same 
 import numpy as np
 import pytest
 
-from jacobi_model import graded, one_sided_jacobi, pivoted_lq
+from jacobi_model import graded, one_sided_jacobi, pivoted_lq, pivoted_lq_blocked
 
 
 @pytest.fixture(scope="module")
@@ -86,3 +86,20 @@ def test_pivoted_lq_of_wide_and_tall_matrices():
         assert np.linalg.norm(X @ X.conj().T - A @ A.conj().T) < 1e-13 * np.linalg.norm(A) ** 2
         if N > R:
             assert np.all(X[:, R:] == 0)  # the Jacobi runs on min(R, N) columns
+
+
+def test_blocked_lq_is_the_same_factorisation():
+    """The panel-blocked form the kernel runs (updates delayed over 8 steps, products corrected
+    for the pending updates) gives the same P L as the step-by-step LQ, to rounding, on square,
+    wide, tall and rank-deficient matrices, with panels that end inside and at kmax."""
+    rng = np.random.default_rng(8)
+    for R, N, b in ((64, 64, 8), (40, 72, 8), (72, 40, 8), (33, 17, 4), (50, 50, 7)):
+        A = rng.normal(size=(R, N)) + 1j * rng.normal(size=(R, N))
+        if (R, N) == (50, 50):
+            U, _, Vh = np.linalg.svd(A)
+            A = (U[:, :20] * np.exp(-np.arange(20) / 3.0)) @ Vh[:20]  # rank 20
+        Xb, Xr = pivoted_lq_blocked(A, b), pivoted_lq(A)
+        scale = np.linalg.norm(A) ** 2
+        assert np.linalg.norm(Xb @ Xb.conj().T - A @ A.conj().T) < 1e-13 * scale
+        if (R, N) != (50, 50):  # full rank: the same pivots, so the same factor
+            assert np.max(np.abs(Xb - Xr)) < 1e-12 * np.sqrt(scale)
