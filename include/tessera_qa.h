@@ -96,8 +96,8 @@ typedef struct tessera_qa_config {
     int kernel_timing;      /* 1 = time every Jacobi-SVD launch with CUDA events (result.svd_ms) */
     int theta_tensor_cores; /* complex64 only: 1 = bond contraction on the tcgen05 tensor cores in split-TF32
                                (three TF32 passes, FP32 accumulators); 0 = CUDA-core FP32 */
-    int jacobi_precondition;/* column-pair Jacobi of theta above 256 rows (up to 512 rows; in a single
-                               instance with jacobi_block 0): 0 = default (on), 1 = on, 2 = off.
+    int jacobi_precondition;/* column-pair Jacobi of theta above 256 rows (up to 512 rows in a batch, 1024
+                               in a single instance with jacobi_block 0): 0 = default (on), 1 = on, 2 = off.
                                On: a row-pivoted Householder LQ of theta (P^T theta = L Q^H) runs first and
                                the Jacobi works on L, which takes fewer sweeps (Drmac-Veselic
                                preconditioning); the results are the same up to rounding */

@@ -751,8 +751,8 @@ private:
         add((void**)&dotout_, sizeof(double) * (1 + n_ + m_));
         add((void**)&amp2_, sizeof(double));
         add((void**)&spins_d_, n_);
-        // candidate rows of the cooperative LQ (theta of 257..512 rows): 8 rows per CTA
-        lq_ok_ = ld_ > 256 && ld_ <= 512;
+        // candidate rows of the cooperative LQ (theta of 257..1024 rows): 8 rows per CTA
+        lq_ok_ = ld_ > 256 && ld_ <= 1024;
         add((void**)&lqc_, lq_ok_ ? lq_coop_scratch_bytes(ld_, (int)es, (ld_ + 7) / 8) : 8);
         TQ_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         TQ_CK(device_alloc((void**)&base_, off));
@@ -851,8 +851,8 @@ private:
         if (!tc_done) launch_theta<T>(M, sch, op, nullptr, work(), dl, dr, stream_);
         // theta above 256 rows (the cooperative column-pair Jacobi): the pivoted LQ first, unless
         // switched off or a block width was forced
-        const bool lq = lq_ok_ && C_.precond != 2 && C_.block == 0 && 2 * dl > 256 && 2 * dl <= 512 &&
-                        2 * dr <= 512;
+        const bool lq = lq_ok_ && C_.precond != 2 && C_.block == 0 && 2 * dl > 256 && 2 * dl <= 1024 &&
+                        2 * dr <= 1024;
         cudaEvent_t a = nullptr, b = nullptr;
         if (lq) {
             cudaEvent_t c = nullptr, d = nullptr;

@@ -129,7 +129,6 @@ template <typename T>
 int launch_svd(const MpsView<T>& mps, int bond, int chi, double tol, int max_sweeps, SvdWork<T> wk,
                int rows_ub, int cols_ub, int block_w, cudaStream_t s, int R = 0, int N = 0, int lq = 0);
 // cooperative row-pivoted LQ of one theta's working copy, in place (lq.cu); rows_ub <= 1024
-// (the engine uses it for 257..512 rows)
 template <typename T>
 void launch_lq_coop(const MpsView<T>& mps, int bond, SvdWork<T> wk, void* scratch, int rows_ub, int cols_ub,
                     cudaStream_t s);

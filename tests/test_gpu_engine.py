@@ -658,6 +658,36 @@ def test_graded_chi256_updates_match_the_oracle(oracle, precond):
         assert np.max(np.abs(ng - no)) < 1e-12 * no.max(), i
 
 
+def test_chi512_updates_with_and_without_the_preconditioner_agree():
+    """1024 x 1024 theta in a single instance: the cooperative LQ runs on 128 CTAs before the
+    cooperative Jacobi.  Three truncating chi=512 updates from the same random MPS (the
+    precision study's generator, n=24, couplings to distance 2) with and without it: the states
+    agree to infidelity 1e-11, the discarded weights to 1e-6 relative, and the preconditioned run
+    takes fewer sweeps.  Without the preconditioner this path is the one the 1024 x 1024 SVD test
+    and the exact chi=1024 anneal check."""
+    from tessera_b200.precision import mps_fidelity as mfid
+    p = instances.chain_range(n=24, dmax=2, seed=4, T=40.0, dt=0.02, chi=512, dist="normal", hzero=True)
+    step = len(p.sa) // 2
+    bonds = []
+    for i, j in zip(p.ei, p.ej):
+        bonds += [k - 1 for k in range(int(j), int(i) + 1, -1)] + [int(i)] + [k for k in range(int(i) + 1, int(j))]
+    q0 = next(q for q, b in enumerate(bonds) if b >= 11)
+    out = {}
+    for precond in (1, 2):
+        s = ffi.Session(p.h, p.ei, p.ej, p.ew, p.sa, p.sb, dt=p.dt, chi=512, jacobi_precondition=precond)
+        s.randomize(4)
+        s.run_gates(step, q0, q0 + 3)
+        r = s.sync()
+        out[precond] = (ffi.checkpoint_to_sites(s.save())[1], r)
+        s.close()
+        assert r.status == 0 and r.two_site_updates == 3
+    (a, ra), (b, rb) = out[1], out[2]
+    assert ra.max_bond == 512 and ra.max_trunc > 1e-6
+    assert 1 - mfid(a, b) < 1e-11
+    assert ra.max_trunc == pytest.approx(rb.max_trunc, rel=1e-6)
+    assert ra.max_sweeps < rb.max_sweeps
+
+
 def test_graph_captured_steps_equal_launched_steps():
     """The batched slot path captures one Trotter step into a CUDA graph and replays it for every
     step when no per-launch timing is asked for; with kernel timing it launches kernel by
