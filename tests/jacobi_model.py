@@ -79,6 +79,59 @@ def one_sided_jacobi(A: np.ndarray, rule: str = "A", tol: float = 1e-13, max_swe
     return sig[order], W[:, order], sweeps, float(np.sqrt(tiny))
 
 
+def tournament_jacobi(A: np.ndarray, bw: int = 4, tol: float = 1e-13, max_sweeps: int = 60) -> int:
+    """Sweeps to convergence in the cooperative kernel's order (k_svd): columns in blocks of bw,
+    a round-robin tournament over the P blocks (P - 1 rounds of P/2 block pairs), a block pair's
+    intra-block pairs in the first round of a sweep, then its bw x bw cross pairs in bw inner
+    rounds; no norm ordering; the rotation and freeze rule F of one_sided_jacobi."""
+    W = np.array(A, dtype=np.complex128, copy=True)
+    R, N = W.shape
+    tiny = max(1e-200, (8.0 * np.sqrt(R) * EPS64) ** 2 * float(np.sum(np.abs(W) ** 2)))
+    P = (N + bw - 1) // bw
+    P += P & 1
+    late = False
+    for sweep in range(max_sweeps):
+        rot = 0
+
+        def pair(p, q):
+            nonlocal rot
+            if p >= N or q >= N:
+                return
+            x, y = W[:, p], W[:, q]
+            v0, v1 = float(np.vdot(x, x).real), float(np.vdot(y, y).real)
+            g = np.vdot(x, y)
+            if late and not (v0 > tiny and v1 > tiny):
+                return
+            if not late and not (max(v0, v1) > tiny and min(v0, v1) > 1e-6 * tiny):
+                return
+            if not (abs(g) ** 2 > tol * tol * v0 * v1):
+                return
+            c, s, e = rotation(v0, v1, float(g.real), float(g.imag))
+            xn = c * x - s * np.conj(e) * y
+            yn = s * e * x + c * y
+            W[:, p], W[:, q] = xn, yn
+            rot += 1
+
+        for r in range(P - 1):
+            for k in range(P // 2):
+                I, J = (P - 1, r) if k == 0 else ((r + k) % (P - 1), (r - k + P - 1) % (P - 1))
+                if r == 0:
+                    for B in (I, J):
+                        for a in range(bw):
+                            for b in range(a + 1, bw):
+                                pair(B * bw + a, B * bw + b)
+                for t in range(bw):
+                    for w in range(bw):
+                        pair(I * bw + w, J * bw + (w + t) % bw)
+        if not late and (rot < 0.1 * N * (N - 1) / 2 or sweep + 1 >= 8 + 3 * int(np.ceil(np.log2(N)))):
+            late = True
+            if rot:
+                continue
+        if rot == 0:
+            return sweep + 1
+    return max_sweeps
+
+
 def pivoted_lq(A: np.ndarray) -> np.ndarray:
     """The preconditioner of tessera_b200/csrc/lq.cu, step for step: a row-pivoted Householder LQ
     P^T A = L Q^H returned as P L in A's own row order.  Step k takes the unpivoted row of largest
